@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark: ms3.bandpass_filter + ms3.whiten on one B200 (or N, weak scaling).
+
+Workload (default): 384 channels x 18,000,000 timepoints (10 min at 30 kHz,
+27.6 GB float32), seeded synthetic recording (correlated noise + 1/f LFP +
+300 biphasic units), filter 300-6000 Hz, freq_wid 1000, chunk geometry of
+T = 16 threads (chunk 120000, FFT window 240000).  One step = the fused
+bandpass -> covariance -> whitening matrix -> apply pass over the whole
+recording, inputs resident in HBM (27.6 GB > 126 MB L2, so no L2 flush is
+needed between steps).
+
+Metric: Gch-samples/s (one ch-sample = one channel at one timepoint of
+output).  `e2e` is the same metric through the C ABI with pinned host
+buffers: the host->device copy of the raw recording and the device->host copy
+of the whitened output happen inside every timed step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FS, FMIN, FMAX, FWID = 30000.0, 300.0, 6000.0, 1000.0
+GEOM_T = 16
+METRIC = "Gch-samples/s bandpass+whiten"
+UNIT = "Gch-samples/s"
+
+SIZES = {
+    # name: (M, N, units, description)
+    "c2": (384, 18_000_000, 300, "384ch x 18M timepoints (10 min @ 30 kHz), config 2"),
+    "c1": (32, 1_800_000, 20, "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1"),
+    "small": (384, 1_200_000, 20, "384ch x 1.2M timepoints (40 s @ 30 kHz), profiling case"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception as e:  # pragma: no cover
+            log("clock sampler unavailable:", e)
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sms.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+# ----------------------------------------------------------------- CPU baseline
+
+def cpu_baseline(M: int, N: int, threads: int):
+    """Times the CPU restatement of the reference (oracle/ref32, OpenMP, the
+    reference's loop structure) on a bounded sample and models the full
+    recording from it.  Returns a cpu_baseline dict (value in Gch-samples/s)."""
+    import numpy as np
+
+    from oracle import ref32
+
+    rng = np.random.default_rng(1)
+    chunk = ref32.chunk_size(M, GEOM_T)
+    T = max(1, threads)
+    # bandpass: T chunks in parallel, one per thread (the reference's omp for)
+    Xs = (10 * rng.standard_normal((T * chunk, M))).astype(np.float32)
+    t0 = time.perf_counter()
+    ref32.bandpass_filter(Xs, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, exec_threads=T)
+    t_bp_round = time.perf_counter() - t0
+    del Xs
+    # whiten passes: per-timepoint cost of each pass on a 2000-timepoint slice (one thread)
+    S = 2000
+    Y = (rng.standard_normal((S, M))).astype(np.float32)
+    t0 = time.perf_counter()
+    C = ref32.whiten_xxt(Y, exec_threads=1)
+    t_xxt = (time.perf_counter() - t0) / S
+    W = np.eye(M)
+    t0 = time.perf_counter()
+    ref32.whiten_apply(Y, W, exec_threads=1)
+    t_apply = (time.perf_counter() - t0) / S
+    # power-iteration matrix: serial O(M^4); timed at M/2 and scaled by 16 for M > 256
+    Mp = M if M <= 256 else M // 2
+    C = np.cov(rng.standard_normal((Mp, 4 * Mp)))
+    t0 = time.perf_counter()
+    ref32.whitening_matrix(C)
+    t_pca = (time.perf_counter() - t0) * (M / Mp) ** 4
+    nchunks = -(-N // chunk)
+    wchunks = -(-N // 100000)
+    rounds = -(-nchunks // T)
+    wrounds = -(-wchunks // T)
+    total = rounds * t_bp_round + wrounds * 100000 * (t_xxt + t_apply) + t_pca
+    value = M * N / total / 1e9
+    return {
+        "value": value, "unit": UNIT, "cores": T, "kind": "port",
+        "sample": (f"ref32 (C++ restatement, OpenMP) on this host: {T} bandpass chunks of {chunk} x {M}ch in "
+                   f"parallel ({t_bp_round:.2f} s), whiten XXt/apply loops on {S} timepoints x {M}ch "
+                   f"({t_xxt * S:.2f} s / {t_apply * S:.2f} s, 1 thread), power-iteration W at M={Mp}"
+                   f"{' scaled x16' if Mp != M else ''}; modelled full run {total:.1f} s for {M}x{N}"),
+    }
+
+
+def run_reference_arm(args, size):
+    M, N, _, desc = SIZES[size]
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    threads = min(threads, int(os.environ.get("MS3_BENCH_CPU_THREADS", "32")))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(M, N, threads)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": M * N / (v * 1e9) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "M": M, "N": N, "geometry_threads": GEOM_T, "freq": [FMIN, FMAX, FWID]},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", default="c2", choices=sorted(SIZES))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stages", action="store_true")
+    args = ap.parse_args()
+
+    if args.impl == "reference":
+        run_reference_arm(args, args.size)
+        return
+
+    import numpy as np
+    import torch
+
+    import mountainsort_b200 as ms
+    from mountainsort_b200 import _lib, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = _lib.load()
+    M, N, K_units, desc = SIZES[args.size]
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    t0 = time.time()
+    X = synth.generate_torch(M, N, fs=FS, K=K_units, seed=1000 + rank, sites=(6, 12) if M >= 64 else (3, 6),
+                             device=dev)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] generated {M}x{N} in {time.time() - t0:.1f} s")
+    pre = torch.empty((N, M), dtype=torch.float32, device=dev)
+
+    def step():
+        ms.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=pre)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.ms3gpu_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = (lib.ms3gpu_launch_count() - l0) // max(1, args.steps)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms_total = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * M * N * args.steps / (ms_total / 1e3) / 1e9
+
+    # ---- stage breakdown (same data, device pointers, CUDA events on the launching stream)
+    stages = {}
+    if not args.no_stages:
+        filt = torch.empty((N, M), dtype=torch.float32, device=dev)
+
+        def timed(fn, reps=2):
+            fn()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / reps
+
+        stages["bandpass_filter"] = timed(lambda: ms.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=GEOM_T,
+                                                                      out=filt))
+        C = ms.whiten_covariance(filt)
+        stages["whiten_covariance"] = timed(lambda: ms.whiten_covariance(filt))
+        stages["whitening_matrix"] = timed(lambda: ms.whitening_matrix(C), reps=1)
+        Wm = ms.whitening_matrix(C)
+        stages["apply_whitening"] = timed(lambda: ms.apply_whitening_matrix(filt, Wm, out=pre))
+        del filt
+
+    # ---- roofline of the dominant stage (HBM bound: algorithmic bytes per ch-sample)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+        hbm_peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    else:
+        hbm_peak, peak_src = 6650.0, "fallback"
+    algo_bytes = {"bandpass_filter": 8, "whiten_covariance": 4, "apply_whitening": 8}
+    roofline = None
+    if stages:
+        dom = max((k for k in stages if k in algo_bytes), key=lambda k: stages[k])
+        achieved = algo_bytes[dom] * M * N / (stages[dom] / 1e3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tpath):
+            tr = json.load(open(tpath)).get(dom)
+            if tr:
+                traffic = tr.get("dram_bytes_per_launch_full")
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                    "algorithmic_bytes_per_ch_sample": algo_bytes[dom], "stage_ms": stages}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        del pre
+        torch.cuda.empty_cache()
+        Xh = torch.empty((N, M), dtype=torch.float32, pin_memory=True)
+        Xh.copy_(X)
+        del X
+        torch.cuda.empty_cache()
+        Ph = torch.empty((N, M), dtype=torch.float32, pin_memory=True)
+        raw_np = Xh.numpy()
+        pre_np = Ph.numpy()
+        ms.bandpass_whiten(raw_np, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=pre_np)  # warm-up
+        if dist:
+            dist.barrier()
+        t1 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ms.bandpass_whiten(raw_np, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=pre_np)
+        el = time.perf_counter() - t1
+        if dist:
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world * M * N * args.e2e_steps / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * M * N,
+               "ms_per_step": el / args.e2e_steps * 1e3, "steps": args.e2e_steps,
+               "timing": "host wall clock around synchronous C-ABI calls (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = min(os.cpu_count() or 1, int(os.environ.get("MS3_BENCH_CPU_THREADS", "32")))
+        cpu = cpu_baseline(M, N, threads)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "M": M, "N": N, "geometry_threads": GEOM_T,
+                       "freq": [FMIN, FMAX, FWID], "l2_flush": "inputs (27.6 GB) larger than L2" if N * M * 4 > 2**30
+                       else "none", "parallelism": f"replicas x{world} (one recording per GPU)"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,149 @@
+/*
+ * ms3gpu -- B200-native ms3.bandpass_filter and ms3.whiten (C ABI).
+ *
+ * The two processors of MountainSort 3's preprocessing front end
+ * (pipelines/mountainsort3.mlp, "sort" script) as a shared library with plain
+ * C entry points: caller-owned buffers, int status codes, no exceptions and
+ * no torch types.  Each entry point is the in-memory form of one reference
+ * processor or of one stage inside it; citations are paths inside the
+ * reference project (flatironinstitute/mountainsort).
+ *
+ * Data layout.  A timeseries of M channels and N timepoints is the .mda
+ * M x N column-major array: element (m, t) at index m + M*t (channel
+ * fastest), float32 unless stated otherwise.  M x M matrices (XXt, W) are
+ * column-major doubles like the reference's Mda: element (i, j) at i + M*j.
+ *
+ * Pointers.  Every buffer argument may be host memory (pageable or pinned)
+ * or device memory of the current CUDA device; the library classifies each
+ * pointer itself.  Host buffers are staged through the device.  Calls return
+ * after the results are complete in the output buffers.
+ *
+ * Streams.  `stream` is a cudaStream_t (NULL = the legacy default stream).
+ * All device work of a call is ordered on that stream.
+ *
+ * Threading.  Calls may come from several host threads; each call uses its
+ * own scratch memory.  Errors are reported per thread by
+ * ms3gpu_last_error().
+ */
+#ifndef MS3GPU_H
+#define MS3GPU_H
+
+#include <stdint.h>
+
+#if defined(MS3GPU_BUILDING) && defined(__GNUC__)
+#define MS3GPU_API __attribute__((visibility("default")))
+#else
+#define MS3GPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference's processors return bool, turned into exit
+ * code 0 / -1 by main (packages/ms3/mountainsort3_main.cpp:817-820). */
+#define MS3GPU_OK 0
+#define MS3GPU_ERR_INVALID -1     /* bad argument (sizes, pointers, options) */
+#define MS3GPU_ERR_CUDA -2        /* a CUDA runtime error */
+#define MS3GPU_ERR_UNSUPPORTED -3 /* a shape the GPU path does not handle */
+#define MS3GPU_ERR_NOMEM -4       /* device memory exhausted */
+
+/* .mda data type codes (packages/ms3/mda/mdaio.h:55-62) used for outputs. */
+#define MS3GPU_DTYPE_FLOAT32 -3
+#define MS3GPU_DTYPE_INT16 -4
+
+/* Bandpass_filter_opts (packages/ms3/p_bandpass_filter.h:21-31), as parsed
+ * by main (packages/ms3/mountainsort3_main.cpp:547-557), plus the thread
+ * count T that the reference's chunk geometry depends on
+ * (p_bandpass_filter.cpp:147-155: T = omp_get_max_threads(), which
+ * --_request_num_threads sets, mountainsort3_main.cpp:428-434). */
+typedef struct ms3gpu_bandpass_opts {
+    double samplerate;
+    double freq_min;
+    double freq_max;
+    double freq_wid;          /* processor default 1000 */
+    double quantization_unit; /* != 0: int16 output of x / quantization_unit */
+    int32_t subsample_factor; /* 0 is treated as 1, like the reference */
+    int32_t num_threads;      /* T of the chunk-size formula; must be >= 1 */
+} ms3gpu_bandpass_opts;
+
+/* Whiten_opts (packages/ms3/p_whiten.h:21-26). */
+typedef struct ms3gpu_whiten_opts {
+    double quantization_unit; /* > 0: int16 output of round(y / quantization_unit) */
+} ms3gpu_whiten_opts;
+
+/* Text of the last error on the calling thread ("" if none). */
+MS3GPU_API const char* ms3gpu_last_error(void);
+
+/* Library version string. */
+MS3GPU_API const char* ms3gpu_version(void);
+
+/* Number of CUDA kernels this library has launched in this process (for
+ * throughput accounting; monotonically increasing). */
+MS3GPU_API uint64_t ms3gpu_launch_count(void);
+
+/* The reference's chunk size for M channels and T threads
+ * (p_bandpass_filter.cpp:147-155); the FFT length is chunk + 120000. */
+MS3GPU_API int64_t ms3gpu_bandpass_chunk_size(int64_t M, int32_t num_threads);
+
+/* Output shape and dtype of ms3.bandpass_filter: M x (N / subsample_factor),
+ * int16 when quantization_unit != 0 else float32 (p_bandpass_filter.cpp:134-142). */
+MS3GPU_API int ms3gpu_bandpass_output_dims(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts,
+                                int64_t* M_out, int64_t* N_out, int32_t* dtype_out);
+
+/* "requirements" answers: the reference's peak-RAM model in MB
+ * (p_bandpass_filter.cpp:157-158, p_whiten.cpp:53-57). */
+MS3GPU_API int ms3gpu_bandpass_requirements(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts,
+                                 double* peak_ram_mb);
+MS3GPU_API int ms3gpu_whiten_requirements(int64_t M, int64_t N, double* peak_ram_mb);
+
+/* ms3.bandpass_filter on a buffer.  Replaces p_bandpass_filter
+ * (packages/ms3/p_bandpass_filter.cpp:115-229): overlap FFT filtering with
+ * the reference's chunk geometry and band kernel (define_kernel, :421-447),
+ * optional subsample (:480-491) and int16 quantization (:207-209).
+ * timeseries_out has the shape and dtype of ms3gpu_bandpass_output_dims().
+ * freq_max == 0 copies the input (:117-119). */
+MS3GPU_API int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                           const ms3gpu_bandpass_opts* opts, void* stream);
+
+/* ms3.whiten on a buffer.  Replaces p_whiten (packages/ms3/p_whiten.cpp:45-206):
+ * XXt/(N-1), the power-iteration whitening matrix (pca.cpp:635-651), W^T x,
+ * 1e-4 rounding and optional int16 quantization.  timeseries_out is M x N,
+ * int16 when quantization_unit > 0 else float32. */
+MS3GPU_API int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                  const ms3gpu_whiten_opts* opts, void* stream);
+
+/* The two processors back to back as mountainsort3.mlp runs them
+ * (ms3.bandpass_filter then ms3.whiten), sharing device buffers.
+ * filt_out (the bandpass output, float32 M x N) may be NULL when the caller
+ * does not need it.  Requires subsample_factor == 1 and
+ * quantization_unit == 0 in bp (the pipeline's settings, whose filtered
+ * output is float32 M x N). */
+MS3GPU_API int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float* filt_out,
+                           void* pre_out, const ms3gpu_bandpass_opts* bp,
+                           const ms3gpu_whiten_opts* wh, void* stream);
+
+/* Stage: whiten pass 1 (p_whiten.cpp:64-118).  XXt = sum_t x_t x_t^T,
+ * divided by N-1 when N > 1, M x M doubles. */
+MS3GPU_API int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt,
+                             void* stream);
+
+/* Stage: whitening_matrix_from_XXt (packages/ms3/pca.cpp:635-651) with
+ * pca_from_XXt (:172-195): M components of 10 power iterations each from
+ * the start vector sin(1..M), deflation (I-cc')XXt(I-cc'), W = C D C' with
+ * D = diag(1/sqrt(sigma)) (0 where sigma == 0).  FP64 on the GPU.
+ * components (M x M) and sigma (M) may be NULL. */
+MS3GPU_API int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* components,
+                            double* sigma, void* stream);
+
+/* Stage: whiten pass 2 (p_whiten.cpp:153-206): out(m1, t) = sum_m2
+ * x(m2, t) W[m1*M + m2], rounded to multiples of 1e-4 (:31-41), then
+ * int16 (int)(y/q + 0.5) when quantization_unit > 0 (:445-451). */
+MS3GPU_API int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N, const double* W,
+                                  double quantization_unit, void* timeseries_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MS3GPU_H */

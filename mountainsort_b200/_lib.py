@@ -1,0 +1,97 @@
+"""ctypes binding of libms3gpu.so (the C ABI declared in include/ms3gpu.h).
+
+There is no fallback: if the shared library is missing or fails to load,
+importing this module raises.  Buffers may be numpy arrays (host memory) or
+torch tensors (host or CUDA); the library classifies each pointer itself.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libms3gpu.so")
+
+OK = 0
+ERR_INVALID = -1
+ERR_CUDA = -2
+ERR_UNSUPPORTED = -3
+ERR_NOMEM = -4
+DTYPE_FLOAT32 = -3
+DTYPE_INT16 = -4
+
+
+class BandpassOpts(ctypes.Structure):
+    """ms3gpu_bandpass_opts (Bandpass_filter_opts, p_bandpass_filter.h:21-31)."""
+    _fields_ = [
+        ("samplerate", ctypes.c_double),
+        ("freq_min", ctypes.c_double),
+        ("freq_max", ctypes.c_double),
+        ("freq_wid", ctypes.c_double),
+        ("quantization_unit", ctypes.c_double),
+        ("subsample_factor", ctypes.c_int32),
+        ("num_threads", ctypes.c_int32),
+    ]
+
+
+class WhitenOpts(ctypes.Structure):
+    """ms3gpu_whiten_opts (Whiten_opts, p_whiten.h:21-26)."""
+    _fields_ = [("quantization_unit", ctypes.c_double)]
+
+
+class Ms3GpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ms3gpu error {code}: {msg}")
+        self.code = code
+
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_dbl = ctypes.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "ms3gpu_last_error": (ctypes.c_char_p, []),
+    "ms3gpu_version": (ctypes.c_char_p, []),
+    "ms3gpu_launch_count": (ctypes.c_uint64, []),
+    "ms3gpu_bandpass_chunk_size": (_i64, [_i64, ctypes.c_int32]),
+    "ms3gpu_bandpass_output_dims": (ctypes.c_int, [_i64, _i64, ctypes.POINTER(BandpassOpts),
+                                                   ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                                   ctypes.POINTER(ctypes.c_int32)]),
+    "ms3gpu_bandpass_requirements": (ctypes.c_int, [_i64, _i64, ctypes.POINTER(BandpassOpts),
+                                                    ctypes.POINTER(_dbl)]),
+    "ms3gpu_whiten_requirements": (ctypes.c_int, [_i64, _i64, ctypes.POINTER(_dbl)]),
+    "ms3gpu_bandpass_filter": (ctypes.c_int, [_vp, _i64, _i64, _vp, ctypes.POINTER(BandpassOpts), _vp]),
+    "ms3gpu_whiten": (ctypes.c_int, [_vp, _i64, _i64, _vp, ctypes.POINTER(WhitenOpts), _vp]),
+    "ms3gpu_bandpass_whiten": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, ctypes.POINTER(BandpassOpts),
+                                              ctypes.POINTER(WhitenOpts), _vp]),
+    "ms3gpu_whiten_covariance": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
+    "ms3gpu_whitening_matrix": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
+    "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, _vp, _vp]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (once).  Raises OSError if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"libms3gpu.so not built: {path} (run python -m mountainsort_b200.build)")
+        L = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return load().ms3gpu_last_error().decode("utf-8", "replace")
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise Ms3GpuError(rc, last_error())

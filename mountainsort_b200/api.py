@@ -1,0 +1,196 @@
+"""Array-level API over the C ABI.
+
+A timeseries of M channels and N timepoints is passed as an (N, M)
+C-contiguous float32 array -- the .mda M x N column-major layout, one row of
+M channels per timepoint.  numpy arrays live in host memory; torch tensors
+may be on the host or on the current CUDA device.  Outputs are allocated
+like the input (numpy -> numpy, torch -> torch on the same device) unless
+`out` is given.  M x M matrices use matrix notation, W[i, j] = W(i, j).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import BandpassOpts, WhitenOpts, check
+
+try:  # torch is optional for host-only use
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def default_num_threads() -> int:
+    """The reference's omp_get_max_threads(): OMP_NUM_THREADS, else the
+    number of hardware threads (p_bandpass_filter.cpp:147)."""
+    v = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
+    if v.isdigit() and int(v) > 0:
+        return int(v)
+    return os.cpu_count() or 1
+
+
+def _is_torch(x) -> bool:
+    return torch is not None and isinstance(x, torch.Tensor)
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if _is_torch(x):
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return x.data_ptr()
+    if not x.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return x.ctypes.data
+
+
+def _stream_ptr(x, stream) -> int:
+    if stream is not None:
+        return int(getattr(stream, "cuda_stream", stream))
+    if _is_torch(x) and x.is_cuda:
+        return torch.cuda.current_stream(x.device).cuda_stream
+    return 0
+
+
+def _as_f32_rows(X):
+    if _is_torch(X):
+        if X.dtype != torch.float32:
+            X = X.float()
+        return X.contiguous()
+    return np.ascontiguousarray(X, dtype=np.float32)
+
+
+def _empty_like(X, shape, dtype):
+    if _is_torch(X):
+        tdt = {np.float32: torch.float32, np.int16: torch.int16, np.float64: torch.float64}[dtype]
+        return torch.empty(shape, dtype=tdt, device=X.device)
+    return np.empty(shape, dtype=dtype)
+
+
+def _mat_in(W, like):
+    """Matrix notation -> the column-major buffer the C ABI expects."""
+    if _is_torch(W):
+        return W.to(torch.float64).t().contiguous()
+    return np.ascontiguousarray(np.asarray(W, dtype=np.float64).T)
+
+
+def _mat_out(buf):
+    return buf.t().contiguous() if _is_torch(buf) else np.ascontiguousarray(buf.T)
+
+
+def bandpass_opts(samplerate, freq_min, freq_max, freq_wid=1000.0, quantization_unit=0.0,
+                  subsample_factor=1, num_threads=None) -> BandpassOpts:
+    return BandpassOpts(float(samplerate), float(freq_min), float(freq_max), float(freq_wid),
+                        float(quantization_unit), int(subsample_factor or 1),
+                        int(num_threads if num_threads else default_num_threads()))
+
+
+def chunk_size(M: int, num_threads: int) -> int:
+    return int(_lib.load().ms3gpu_bandpass_chunk_size(M, num_threads))
+
+
+def bandpass_filter(X, samplerate, freq_min, freq_max, freq_wid=1000.0, quantization_unit=0.0,
+                    subsample_factor=1, num_threads=None, out=None, stream=None):
+    """ms3.bandpass_filter (packages/ms3/p_bandpass_filter.cpp:115-229) on an
+    (N, M) array; returns (N // subsample_factor, M) float32, or int16 when
+    quantization_unit != 0."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    o = bandpass_opts(samplerate, freq_min, freq_max, freq_wid, quantization_unit, subsample_factor,
+                      num_threads)
+    Mo, No, dt = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    check(L.ms3gpu_bandpass_output_dims(M, N, ctypes.byref(o), ctypes.byref(Mo), ctypes.byref(No),
+                                        ctypes.byref(dt)))
+    if out is None:
+        out = _empty_like(X, (No.value, Mo.value), np.int16 if dt.value == _lib.DTYPE_INT16 else np.float32)
+    check(L.ms3gpu_bandpass_filter(_ptr(X), M, N, _ptr(out), ctypes.byref(o), _stream_ptr(X, stream)))
+    return out
+
+
+def whiten(X, quantization_unit=0.0, out=None, stream=None):
+    """ms3.whiten (packages/ms3/p_whiten.cpp:45-206) on an (N, M) array."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    if out is None:
+        out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
+    o = WhitenOpts(float(quantization_unit))
+    check(L.ms3gpu_whiten(_ptr(X), M, N, _ptr(out), ctypes.byref(o), _stream_ptr(X, stream)))
+    return out
+
+
+def bandpass_whiten(X, samplerate, freq_min, freq_max, freq_wid=1000.0, num_threads=None,
+                    quantization_unit=0.0, filt_out=None, out=None, want_filt=False, stream=None):
+    """ms3.bandpass_filter followed by ms3.whiten, as mountainsort3.mlp runs
+    them.  Returns pre, or (filt, pre) when want_filt or filt_out is given."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    bp = bandpass_opts(samplerate, freq_min, freq_max, freq_wid, 0.0, 1, num_threads)
+    wh = WhitenOpts(float(quantization_unit))
+    if want_filt and filt_out is None:
+        filt_out = _empty_like(X, (N, M), np.float32)
+    if out is None:
+        out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
+    check(L.ms3gpu_bandpass_whiten(_ptr(X), M, N, _ptr(filt_out), _ptr(out), ctypes.byref(bp),
+                                   ctypes.byref(wh), _stream_ptr(X, stream)))
+    return (filt_out, out) if filt_out is not None else out
+
+
+def whiten_covariance(X, stream=None):
+    """XXt = sum_t x_t x_t^T / (N-1) (p_whiten.cpp:64-118), M x M float64."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    buf = _empty_like(X, (M, M), np.float64)
+    check(L.ms3gpu_whiten_covariance(_ptr(X), M, N, _ptr(buf), _stream_ptr(X, stream)))
+    return _mat_out(buf)
+
+
+def whitening_matrix(XXt, stream=None, return_components=False):
+    """whitening_matrix_from_XXt (pca.cpp:635-651).  Returns W, or
+    (W, components, sigma) when return_components."""
+    L = _lib.load()
+    C = _mat_in(XXt, XXt)
+    M = C.shape[0]
+    W = _empty_like(C, (M, M), np.float64)
+    comps = _empty_like(C, (M, M), np.float64) if return_components else None
+    sig = _empty_like(C, (M,), np.float64) if return_components else None
+    check(L.ms3gpu_whitening_matrix(_ptr(C), M, _ptr(W), _ptr(comps), _ptr(sig), _stream_ptr(C, stream)))
+    if return_components:
+        return _mat_out(W), _mat_out(comps), sig
+    return _mat_out(W)
+
+
+def apply_whitening_matrix(X, W, quantization_unit=0.0, out=None, stream=None):
+    """Whiten pass 2 (p_whiten.cpp:153-206) with a given W."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    Wc = _mat_in(W, X)
+    if out is None:
+        out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
+    check(L.ms3gpu_apply_whitening_matrix(_ptr(X), M, N, _ptr(Wc), float(quantization_unit), _ptr(out),
+                                          _stream_ptr(X, stream)))
+    return out
+
+
+def requirements(processor: str, M: int, N: int, **params) -> float:
+    """The processor's peak-RAM model in MB (its "requirements" answer)."""
+    L = _lib.load()
+    mb = ctypes.c_double()
+    if processor == "ms3.bandpass_filter":
+        o = bandpass_opts(params.get("samplerate", 0), params.get("freq_min", 0), params.get("freq_max", 0),
+                          params.get("freq_wid", 1000), params.get("quantization_unit", 0),
+                          params.get("subsample_factor", 1), params.get("num_threads"))
+        check(L.ms3gpu_bandpass_requirements(M, N, ctypes.byref(o), ctypes.byref(mb)))
+    elif processor == "ms3.whiten":
+        check(L.ms3gpu_whiten_requirements(M, N, ctypes.byref(mb)))
+    else:
+        raise ValueError(f"unknown processor {processor}")
+    return mb.value

@@ -1,0 +1,491 @@
+// ms3.bandpass_filter on the GPU.
+//
+// Reference: packages/ms3/p_bandpass_filter.cpp:115-229.  The recording is
+// cut into chunks of `chunk` timepoints (chunk from the reference's formula,
+// :147-155); chunk c is filtered inside the window
+//     [c*chunk - 60000, c*chunk + chunk + 60000)           (L = chunk + 120000)
+// zero-padded outside [0, N) (mda/diskreadmda32.cpp:615-661), by an L-point
+// DFT, multiplication with kernel[k]/L (define_kernel, :421-447, DC bin exactly
+// 0 when freq_min != 0) and the inverse DFT; the middle `chunk` samples are
+// kept (:198).  Keeping this geometry exactly is what makes the output match
+// the reference: the DC kill subtracts H(0)*mean(window) per window and the
+// circular wrap of the long filter tail depends on L.
+//
+// GPU formulation ("four-step" FFT, L = L1 * L2, window index n = L2*n1 + n2,
+// frequency k = k1 + L1*k2):
+//   F1  bp_cols_forward : for each n2, the L1-point DFT over n1 of the window
+//                         column -> A[k1][n2]
+//   F2  bp_rows_filter  : for each k1, twiddle w_L^{n2 k1}, L2-point DFT over
+//                         n2 -> k2, multiply by kernel[k1 + L1 k2]/L, inverse
+//                         L2-point DFT, twiddle w_L^{-n2 k1}   (in place)
+//   F3  bp_cols_inverse : for each n2, the inverse L1-point DFT over k1 -> n1,
+//                         keep the samples inside [60000, 60000 + chunk),
+//                         subsample / quantize, store.
+// Two real channels (2p, 2p+1) travel as one complex signal x_2p + i x_2p+1:
+// the band kernel is real and even (kernel[k] == kernel[L-k] for even L), so
+// the real and imaginary parts of the inverse transform are the two filtered
+// channels.  A unit of work is (window, group of G channel pairs); its
+// spectrum lives in a scratch slab of L*G complex values between F1 and F3.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "bandpass.h"
+#include "common.cuh"
+#include "fft_block.cuh"
+
+namespace ms3gpu {
+
+namespace {
+
+constexpr int64_t kOverlap = 60000;
+constexpr int kThreads = 256;
+constexpr size_t kSmemBudget = 200 * 1024;
+
+struct Geom {
+    int64_t M, N;        // input shape
+    int64_t P;           // complex signals: channel pairs (or channels when unpaired)
+    int paired;          // 1: two channels per complex signal
+    int m_even;          // M even (pairs load as aligned float2)
+    int log2G;           // signals per unit = 1 << log2G
+    int ngroups;
+    int64_t L, L1, L2;
+    int64_t chunk;
+    int sub;
+    int64_t N2;          // output timepoints
+    int out_i16;
+    double qscale;       // 1 / quantization_unit
+};
+
+// ---------------------------------------------------------------- kernels
+
+__device__ __forceinline__ float2 load_signal(const float* __restrict__ raw, const Geom& g, int64_t t,
+                                              int64_t s) {
+    if (t < 0 || t >= g.N || s >= g.P) return make_float2(0.f, 0.f);
+    const float* row = raw + t * g.M;
+    if (!g.paired) return make_float2(row[s], 0.f);
+    const int64_t m0 = 2 * s;
+    if (g.m_even) return *reinterpret_cast<const float2*>(row + m0);
+    return make_float2(row[m0], (m0 + 1 < g.M) ? row[m0 + 1] : 0.f);
+}
+
+__device__ __forceinline__ void load_plan(SubFft& dst, const SubFft& src) {
+    int* d = reinterpret_cast<int*>(&dst);
+    const int* s = reinterpret_cast<const int*>(&src);
+    for (int i = threadIdx.x; i < (int)(sizeof(SubFft) / sizeof(int)); i += blockDim.x) d[i] = s[i];
+}
+
+// F1: forward L1-point transforms of the window columns.
+__global__ void __launch_bounds__(kThreads) bp_cols_forward(const float* __restrict__ raw,
+                                                            float2* __restrict__ scratch, Geom g,
+                                                            SubFft P1, const float2* __restrict__ tw1,
+                                                            int64_t unit0) {
+    extern __shared__ float4 smem_f4[];
+    float2* smem = reinterpret_cast<float2*>(smem_f4);
+    __shared__ SubFft plan;
+    const int G = 1 << g.log2G;
+    const int n1len = (int)g.L1;
+    float2* bufA = smem;
+    float2* bufB = bufA + (size_t)n1len * G;
+    float2* twS = bufB + (size_t)n1len * G;
+    load_plan(plan, P1);
+    for (int i = threadIdx.x; i < P1.twlen; i += blockDim.x) twS[i] = tw1[i];
+
+    const int n2 = blockIdx.x;
+    const int64_t unit = unit0 + blockIdx.y;
+    const int64_t c = unit / g.ngroups;
+    const int grp = (int)(unit % g.ngroups);
+    const int64_t t0 = c * g.chunk - kOverlap + n2;
+    for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
+        const int n1 = idx >> g.log2G;
+        const int gi = idx & (G - 1);
+        bufA[idx] = load_signal(raw, g, t0 + (int64_t)n1 * g.L2, (int64_t)grp * G + gi);
+    }
+    __syncthreads();
+    float2* res = fft_smem<false>(bufA, bufB, twS, plan, g.log2G);
+    float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
+    for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
+        const int k1 = idx >> g.log2G;
+        const int gi = idx & (G - 1);
+        slab[(((size_t)k1 * g.L2 + n2) << g.log2G) + gi] = res[idx];
+    }
+}
+
+// F2: per k1 row: twiddle, L2-point forward DFT, band kernel, inverse DFT,
+// inverse twiddle.
+__global__ void __launch_bounds__(kThreads) bp_rows_filter(float2* __restrict__ scratch, Geom g, SubFft P2,
+                                                           const float2* __restrict__ tw2,
+                                                           const float2* __restrict__ twL,
+                                                           const float* __restrict__ kern) {
+    extern __shared__ float4 smem_f4[];
+    float2* smem = reinterpret_cast<float2*>(smem_f4);
+    __shared__ SubFft plan;
+    const int G = 1 << g.log2G;
+    const int n2len = (int)g.L2;
+    float2* bufA = smem;
+    float2* bufB = bufA + (size_t)n2len * G;
+    float2* twS = bufB + (size_t)n2len * G;
+    load_plan(plan, P2);
+    for (int i = threadIdx.x; i < P2.twlen; i += blockDim.x) twS[i] = tw2[i];
+
+    const int k1 = blockIdx.x;
+    float2* row = scratch + (size_t)blockIdx.y * (size_t)(g.L * G) + (((size_t)k1 * g.L2) << g.log2G);
+    const float2* twrow = twL + (size_t)k1 * g.L2;
+    const float* krow = kern + (size_t)k1 * g.L2;
+    for (int idx = threadIdx.x; idx < n2len * G; idx += blockDim.x) {
+        const int n2 = idx >> g.log2G;
+        bufA[idx] = cmul(row[idx], twrow[n2]);
+    }
+    __syncthreads();
+    float2* res = fft_smem<false>(bufA, bufB, twS, plan, g.log2G);
+    float2* other = (res == bufA) ? bufB : bufA;
+    for (int idx = threadIdx.x; idx < n2len * G; idx += blockDim.x) {
+        const float kv = krow[idx >> g.log2G];
+        float2 v = res[idx];
+        res[idx] = make_float2(v.x * kv, v.y * kv);
+    }
+    __syncthreads();
+    float2* res2 = fft_smem<true>(res, other, twS, plan, g.log2G);
+    for (int idx = threadIdx.x; idx < n2len * G; idx += blockDim.x) {
+        const int n2 = idx >> g.log2G;
+        float2 w = twrow[n2];
+        w.y = -w.y;
+        row[idx] = cmul(res2[idx], w);
+    }
+}
+
+// F3: inverse L1-point transforms of the columns, trim, subsample, quantize,
+// store.
+__global__ void __launch_bounds__(kThreads) bp_cols_inverse(const float2* __restrict__ scratch,
+                                                            void* __restrict__ out, Geom g, SubFft P1,
+                                                            const float2* __restrict__ tw1,
+                                                            int64_t unit0) {
+    extern __shared__ float4 smem_f4[];
+    float2* smem = reinterpret_cast<float2*>(smem_f4);
+    __shared__ SubFft plan;
+    const int G = 1 << g.log2G;
+    const int n1len = (int)g.L1;
+    float2* bufA = smem;
+    float2* bufB = bufA + (size_t)n1len * G;
+    float2* twS = bufB + (size_t)n1len * G;
+    load_plan(plan, P1);
+    for (int i = threadIdx.x; i < P1.twlen; i += blockDim.x) twS[i] = tw1[i];
+
+    const int n2 = blockIdx.x;
+    const int64_t unit = unit0 + blockIdx.y;
+    const int64_t c = unit / g.ngroups;
+    const int grp = (int)(unit % g.ngroups);
+    const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
+    for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
+        const int k1 = idx >> g.log2G;
+        const int gi = idx & (G - 1);
+        bufA[idx] = slab[(((size_t)k1 * g.L2 + n2) << g.log2G) + gi];
+    }
+    __syncthreads();
+    float2* res = fft_smem<true>(bufA, bufB, twS, plan, g.log2G);
+    const int64_t nsub = g.chunk / g.sub;
+    const int64_t ot0 = (c * g.chunk) / g.sub;
+    for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
+        const int n1 = idx >> g.log2G;
+        const int gi = idx & (G - 1);
+        const int64_t s = (int64_t)grp * G + gi;
+        if (s >= g.P) continue;
+        const int64_t j = (int64_t)n1 * g.L2 + n2 - kOverlap;
+        if (j < 0 || j >= g.chunk) continue;
+        if (j % g.sub) continue;
+        const int64_t jj = j / g.sub;
+        if (jj >= nsub) continue;
+        const int64_t ot = ot0 + jj;
+        if (ot >= g.N2) continue;
+        const float2 v = res[idx];
+        const int64_t m0 = g.paired ? 2 * s : s;
+        const bool has2 = g.paired && (m0 + 1 < g.M);
+        const size_t o = (size_t)(ot * g.M + m0);
+        if (g.out_i16) {
+            int16_t* o16 = static_cast<int16_t*>(out);
+            o16[o] = x86_float_to_int16((float)((double)v.x * g.qscale));
+            if (has2) o16[o + 1] = x86_float_to_int16((float)((double)v.y * g.qscale));
+        } else {
+            float* of = static_cast<float*>(out);
+            if (has2 && g.m_even) {
+                *reinterpret_cast<float2*>(of + o) = v;
+            } else {
+                of[o] = v.x;
+                if (has2) of[o + 1] = v.y;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- plans
+
+int max_prime_factor(int64_t n) {
+    int64_t m = 1;
+    for (int64_t p = 2; p * p <= n; p++)
+        while (n % p == 0) { m = std::max(m, p); n /= p; }
+    if (n > 1) m = std::max(m, n);
+    return (int)m;
+}
+
+SubFft make_subfft(int n, std::vector<float2>& tw) {
+    SubFft P{};
+    P.n = n;
+    std::vector<int> rad;
+    int m = n;
+    while (m % 8 == 0) { rad.push_back(8); m /= 8; }
+    while (m % 4 == 0) { rad.push_back(4); m /= 4; }
+    while (m % 2 == 0) { rad.push_back(2); m /= 2; }
+    while (m % 5 == 0) { rad.push_back(5); m /= 5; }
+    while (m % 3 == 0) { rad.push_back(3); m /= 3; }
+    for (int f = 7; f <= m; f += 2)
+        while (m % f == 0) { rad.push_back(f); m /= f; }
+    if ((int)rad.size() > kMaxPasses) throw_unsupported("FFT factor has too many passes");
+    P.npass = (int)rad.size();
+    int64_t p = 1;
+    tw.clear();
+    for (int s = 0; s < P.npass; s++) {
+        const int r = rad[s];
+        P.radix[s] = r;
+        P.p[s] = (int)p;
+        P.twoff[s] = (int)tw.size();
+        for (int64_t k = 0; k < p; k++)
+            for (int q = 0; q < r; q++) {
+                const int64_t num = (q * k) % (p * r);
+                const double a = -2.0 * M_PI * (double)num / (double)(p * r);
+                tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+            }
+        p *= r;
+    }
+    if (n == 1) P.npass = 0;
+    P.twlen = (int)tw.size();
+    return P;
+}
+
+size_t smem_bytes_for(int n, int G, int twlen) {
+    return (size_t)2 * n * G * sizeof(float2) + (size_t)twlen * sizeof(float2);
+}
+
+// Device-resident tables for one (L, filter) combination.
+struct BandpassPlan {
+    int device = -1;
+    int64_t L = 0, L1 = 0, L2 = 0;
+    int paired = 1;
+    SubFft P1{}, P2{};
+    float2* tw1 = nullptr;  // P1 twiddles
+    float2* tw2 = nullptr;  // P2 twiddles
+    float2* twL = nullptr;  // [k1][n2] exp(-2 pi i n2 k1 / L)
+    float* kern = nullptr;  // [k1][k2] kernel[k1 + L1 k2] / L
+    ~BandpassPlan() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (device >= 0) cudaSetDevice(device);
+        cudaFree(tw1);
+        cudaFree(tw2);
+        cudaFree(twL);
+        cudaFree(kern);
+        if (cur >= 0) cudaSetDevice(cur);
+    }
+};
+
+// Choose L = L1 * L2 with both factors built from primes <= kMaxGenericRadix,
+// minimising the larger factor.
+bool factor_window(int64_t L, int64_t& L1, int64_t& L2) {
+    int64_t best = -1;
+    for (int64_t a = 1; a * a <= L; a++) {
+        if (L % a) continue;
+        const int64_t b = L / a;
+        if (max_prime_factor(a) > kMaxGenericRadix || max_prime_factor(b) > kMaxGenericRadix) continue;
+        if (best < 0 || b < best) { best = b; L1 = a; L2 = b; }
+    }
+    if (best < 0) return false;
+    // the longer transform goes to the contiguous (row) pass
+    if (L1 > L2) std::swap(L1, L2);
+    return true;
+}
+
+std::shared_ptr<BandpassPlan> build_plan(int64_t L, double fs, double fmin, double fmax, double fwid) {
+    auto plan = std::make_shared<BandpassPlan>();
+    MS3_CUDA(cudaGetDevice(&plan->device));
+    plan->L = L;
+    if (!factor_window(L, plan->L1, plan->L2))
+        throw_unsupported("FFT window length " + std::to_string(L) +
+                          " has a prime factor above 64; not supported by the GPU path");
+    if (plan->L2 > 16384)
+        throw_unsupported("FFT window length " + std::to_string(L) + " needs a factor above 16384");
+    const int64_t L1 = plan->L1, L2 = plan->L2;
+    std::vector<float2> tw1, tw2;
+    plan->P1 = make_subfft((int)L1, tw1);
+    plan->P2 = make_subfft((int)L2, tw2);
+
+    // band kernel (define_kernel, p_bandpass_filter.cpp:421-447)
+    std::vector<double> K((size_t)L);
+    {
+        const double T = L / fs;
+        const double df = 1 / T;
+        for (int64_t i = 0; i < L; i++) {
+            const double fgrid = (i <= (L + 1) / 2) ? df * i : df * (i - L);
+            const double absf = std::fabs(fgrid);
+            double val = 1.0;
+            if (fmin != 0) {
+                if (i == 0)
+                    val = 0.0;
+                else
+                    val *= (1 + std::erf(3.0 * (absf - fmin) / fmin)) / 2;
+            }
+            if (fmax != 0) val *= (1 - std::erf((absf - fmax) / fwid)) / 2;
+            K[(size_t)i] = std::sqrt(val);
+        }
+    }
+    // Two channels can share one complex transform only if the kernel is even.
+    plan->paired = 1;
+    for (int64_t i = 1; i < L; i++)
+        if (K[(size_t)i] != K[(size_t)(L - i)]) { plan->paired = 0; break; }
+
+    const double factor = 1.0 / L;
+    std::vector<float> kern((size_t)L);
+    std::vector<float2> twL((size_t)L);
+    for (int64_t k1 = 0; k1 < L1; k1++)
+        for (int64_t j = 0; j < L2; j++) {
+            kern[(size_t)(k1 * L2 + j)] = (float)(K[(size_t)(k1 + L1 * j)] * factor);
+            const double a = -2.0 * M_PI * (double)(j * k1) / (double)L;
+            twL[(size_t)(k1 * L2 + j)] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+    MS3_CUDA(cudaMalloc(&plan->tw1, std::max<size_t>(1, tw1.size()) * sizeof(float2)));
+    MS3_CUDA(cudaMalloc(&plan->tw2, std::max<size_t>(1, tw2.size()) * sizeof(float2)));
+    MS3_CUDA(cudaMalloc(&plan->twL, (size_t)L * sizeof(float2)));
+    MS3_CUDA(cudaMalloc(&plan->kern, (size_t)L * sizeof(float)));
+    if (!tw1.empty()) MS3_CUDA(cudaMemcpy(plan->tw1, tw1.data(), tw1.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    if (!tw2.empty()) MS3_CUDA(cudaMemcpy(plan->tw2, tw2.data(), tw2.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    MS3_CUDA(cudaMemcpy(plan->twL, twL.data(), (size_t)L * sizeof(float2), cudaMemcpyHostToDevice));
+    MS3_CUDA(cudaMemcpy(plan->kern, kern.data(), (size_t)L * sizeof(float), cudaMemcpyHostToDevice));
+    return plan;
+}
+
+std::mutex g_plan_mu;
+std::map<std::tuple<int, int64_t, double, double, double, double>, std::shared_ptr<BandpassPlan>> g_plans;
+
+std::shared_ptr<BandpassPlan> get_plan(int64_t L, double fs, double fmin, double fmax, double fwid) {
+    int dev = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    auto key = std::make_tuple(dev, L, fs, fmin, fmax, fwid);
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plans.find(key);
+    if (it != g_plans.end()) return it->second;
+    if (g_plans.size() >= 16) g_plans.clear();
+    auto p = build_plan(L, fs, fmin, fmax, fwid);
+    g_plans[key] = p;
+    return p;
+}
+
+size_t env_size(const char* name, size_t dflt) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    return (size_t)std::strtoull(v, nullptr, 10);
+}
+
+}  // namespace
+
+int64_t bandpass_chunk_size(int64_t M, int64_t num_threads) {
+    // p_bandpass_filter.cpp:147-155
+    const int overhead = 6;
+    const int64_t overlap_size = kOverlap;
+    const int64_t min_chunk_size = overlap_size * 2;
+    const double target_ram_bytes = 1.0 * (1024 * 1024 * 1024);
+    const double target_chunk_size =
+        target_ram_bytes / (overhead * sizeof(float) * M * num_threads) - 2 * overlap_size;
+    int64_t chunk_size = (int64_t)(target_chunk_size);
+    if (chunk_size < min_chunk_size) chunk_size = min_chunk_size;
+    return chunk_size;
+}
+
+void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
+                     cudaStream_t stream) {
+    const int sub = bp.subsample_factor ? bp.subsample_factor : 1;
+    if (sub < 1) throw_invalid("subsample_factor must be >= 1");
+    const int64_t N2 = N / sub;
+    const bool out_i16 = bp.quantization_unit != 0;
+    if (bp.freq_max == 0) {
+        // p_bandpass_filter.cpp:117-119: the input file is copied unchanged.
+        if (M * N > 0)
+            MS3_CUDA(cudaMemcpyAsync(out, raw, sizeof(float) * (size_t)(M * N), cudaMemcpyDeviceToDevice, stream));
+        return;
+    }
+    if (M <= 0 || N2 <= 0) return;
+    if (bp.num_threads < 1) throw_invalid("num_threads must be >= 1");
+    const int64_t chunk = bandpass_chunk_size(M, bp.num_threads);
+    const int64_t L = chunk + 2 * kOverlap;
+    auto plan = get_plan(L, bp.samplerate, bp.freq_min, bp.freq_max, bp.freq_wid);
+
+    Geom g{};
+    g.M = M;
+    g.N = N;
+    g.paired = plan->paired;
+    g.P = g.paired ? (M + 1) / 2 : M;
+    g.m_even = (M % 2 == 0);
+    g.L = L;
+    g.L1 = plan->L1;
+    g.L2 = plan->L2;
+    g.chunk = chunk;
+    g.sub = sub;
+    g.N2 = N2;
+    g.out_i16 = out_i16 ? 1 : 0;
+    g.qscale = out_i16 ? 1.0 / bp.quantization_unit : 1.0;
+    // signals per unit: up to 16, limited by the shared-memory budget
+    int log2G = 4;
+    while (log2G > 0 && ((int64_t(1) << (log2G - 1)) >= g.P)) log2G--;
+    while (log2G > 0 && (smem_bytes_for((int)plan->L1, 1 << log2G, plan->P1.twlen) > kSmemBudget ||
+                         smem_bytes_for((int)plan->L2, 1 << log2G, plan->P2.twlen) > kSmemBudget))
+        log2G--;
+    const size_t sm1 = smem_bytes_for((int)plan->L1, 1 << log2G, plan->P1.twlen);
+    const size_t sm2 = smem_bytes_for((int)plan->L2, 1 << log2G, plan->P2.twlen);
+    if (sm1 > kSmemBudget || sm2 > kSmemBudget)
+        throw_unsupported("FFT factors of L=" + std::to_string(L) + " exceed shared memory");
+    g.log2G = log2G;
+    const int G = 1 << log2G;
+    g.ngroups = (int)ceil_div(g.P, G);
+    const int64_t nchunks = ceil_div(N, chunk);
+    const int64_t units = nchunks * g.ngroups;
+    const size_t unit_bytes = (size_t)L * G * sizeof(float2);
+    const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 96) << 20;
+    int64_t per_batch = std::max<int64_t>(1, (int64_t)(budget / unit_bytes));
+    per_batch = std::min<int64_t>(per_batch, std::min<int64_t>(units, 65535));
+
+    static bool attrs_set[64] = {false};
+    {
+        int dev = 0;
+        MS3_CUDA(cudaGetDevice(&dev));
+        if (dev < 64 && !attrs_set[dev]) {
+            MS3_CUDA(cudaFuncSetAttribute(bp_cols_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+            MS3_CUDA(cudaFuncSetAttribute(bp_rows_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+            MS3_CUDA(cudaFuncSetAttribute(bp_cols_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+            attrs_set[dev] = true;
+        }
+    }
+    // Gaps between subsampled chunks stay zero, as in the preallocated file.
+    if (sub > 1 && chunk % sub != 0) {
+        const size_t esz = out_i16 ? 2 : 4;
+        MS3_CUDA(cudaMemsetAsync(out, 0, esz * (size_t)(M * N2), stream));
+    }
+    DevBuf scratch((size_t)per_batch * unit_bytes, stream);
+    for (int64_t u0 = 0; u0 < units; u0 += per_batch) {
+        const int64_t nb = std::min<int64_t>(per_batch, units - u0);
+        dim3 g1((unsigned)plan->L2, (unsigned)nb);
+        dim3 g2((unsigned)plan->L1, (unsigned)nb);
+        bp_cols_forward<<<g1, kThreads, sm1, stream>>>(raw, scratch.as<float2>(), g, plan->P1, plan->tw1, u0);
+        MS3_LAUNCH_CHECK();
+        bp_rows_filter<<<g2, kThreads, sm2, stream>>>(scratch.as<float2>(), g, plan->P2, plan->tw2, plan->twL,
+                                                     plan->kern);
+        MS3_LAUNCH_CHECK();
+        bp_cols_inverse<<<g1, kThreads, sm1, stream>>>(scratch.as<float2>(), out, g, plan->P1, plan->tw1, u0);
+        MS3_LAUNCH_CHECK();
+    }
+}
+
+}  // namespace ms3gpu

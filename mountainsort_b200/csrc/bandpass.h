@@ -1,0 +1,23 @@
+// Internal interface of the bandpass stage (device pointers only).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ms3gpu {
+
+struct BandpassParams {
+    double samplerate = 0, freq_min = 0, freq_max = 0, freq_wid = 1000, quantization_unit = 0;
+    int subsample_factor = 1;
+    int num_threads = 1;
+};
+
+// The reference's chunk size (p_bandpass_filter.cpp:147-155).
+int64_t bandpass_chunk_size(int64_t M, int64_t num_threads);
+
+// raw: device (N, M) float32 rows; out: device M x (N/sub), float32 or int16.
+void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
+                     cudaStream_t stream);
+
+}  // namespace ms3gpu

@@ -1,0 +1,404 @@
+// C ABI of libms3gpu (declared in include/ms3gpu.h).
+//
+// Each entry point validates its arguments, classifies every buffer as host
+// or device memory, stages host buffers through stream-ordered device
+// allocations, runs the device stages, copies results back and synchronises
+// the stream.  C++ exceptions never cross the boundary: they become status
+// codes plus the per-thread text returned by ms3gpu_last_error().
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "bandpass.h"
+#include "common.cuh"
+#include "ms3gpu.h"
+#include "whiten.h"
+
+namespace ms3gpu {
+
+namespace {
+thread_local std::string g_last_error;
+std::mutex g_pool_mu;
+bool g_pool_configured[64] = {false};
+}  // namespace
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    cudaGetLastError();  // clear a non-sticky error so later calls can proceed
+    const int code = (e == cudaErrorMemoryAllocation) ? MS3GPU_ERR_NOMEM : MS3GPU_ERR_CUDA;
+    throw Error(code, std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+                          ") in " + what + " at " + file + ":" + std::to_string(line));
+}
+
+[[noreturn]] void throw_invalid(const std::string& msg) { throw Error(MS3GPU_ERR_INVALID, msg); }
+
+static unsigned long long g_launches = 0;
+void count_launch() { __atomic_fetch_add(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+[[noreturn]] void throw_unsupported(const std::string& msg) { throw Error(MS3GPU_ERR_UNSUPPORTED, msg); }
+
+// Test hook: MS3GPU_FAIL_ALLOC_AFTER=n makes the (n+1)-th device allocation
+// of the process fail as if the device were out of memory.
+static long long fail_alloc_countdown() {
+    static long long v = [] {
+        const char* s = std::getenv("MS3GPU_FAIL_ALLOC_AFTER");
+        return (s && *s) ? std::atoll(s) : -1LL;
+    }();
+    return v;
+}
+static long long g_alloc_count = 0;
+
+static void configure_pool() {
+    int dev = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 64 && !g_pool_configured[dev]) {
+        cudaMemPool_t pool;
+        MS3_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        uint64_t thr = std::numeric_limits<uint64_t>::max();
+        MS3_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        g_pool_configured[dev] = true;
+    }
+}
+
+void DevBuf::alloc(size_t bytes, cudaStream_t s) {
+    release();
+    s_ = s;
+    if (bytes == 0) return;
+    const long long lim = fail_alloc_countdown();
+    if (lim >= 0 && __atomic_fetch_add(&g_alloc_count, 1, __ATOMIC_RELAXED) >= lim)
+        throw Error(MS3GPU_ERR_NOMEM, "device allocation of " + std::to_string(bytes) +
+                                          " bytes failed (MS3GPU_FAIL_ALLOC_AFTER test hook)");
+    configure_pool();
+    MS3_CUDA(cudaMallocAsync(&p_, bytes, s));
+    n_ = bytes;
+}
+
+void DevBuf::release() {
+    if (p_) cudaFreeAsync(p_, s_);
+    p_ = nullptr;
+    n_ = 0;
+}
+
+namespace {
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// A read-only view of a caller buffer on the device.
+struct InView {
+    const void* ptr = nullptr;
+    DevBuf own;
+};
+
+void stage_in(InView& v, const void* p, size_t bytes, cudaStream_t s) {
+    if (bytes == 0 || is_device_ptr(p)) {
+        v.ptr = p;
+        return;
+    }
+    v.own.alloc(bytes, s);
+    MS3_CUDA(cudaMemcpyAsync(v.own.get(), p, bytes, cudaMemcpyHostToDevice, s));
+    v.ptr = v.own.get();
+}
+
+// A writable device buffer for a caller output; copied back by finish().
+struct OutView {
+    void* user = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool host = false;
+    DevBuf own;
+    void setup(void* p, size_t b, cudaStream_t s, DevBuf* reuse = nullptr) {
+        user = p;
+        bytes = b;
+        if (b == 0 || is_device_ptr(p)) {
+            ptr = p;
+            return;
+        }
+        host = true;
+        if (reuse && reuse->get() && reuse->size() >= b) {
+            ptr = reuse->get();
+        } else {
+            own.alloc(b, s);
+            ptr = own.get();
+        }
+    }
+    void finish(cudaStream_t s) {
+        if (host && bytes) MS3_CUDA(cudaMemcpyAsync(user, ptr, bytes, cudaMemcpyDeviceToHost, s));
+    }
+};
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return MS3GPU_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host memory exhausted";
+        return MS3GPU_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return MS3GPU_ERR_INVALID;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return MS3GPU_ERR_INVALID;
+    }
+}
+
+void check_shape(int64_t M, int64_t N) {
+    if (M < 0 || N < 0) throw_invalid("negative dimension (M=" + std::to_string(M) + ", N=" + std::to_string(N) + ")");
+    if (M > 0 && N > std::numeric_limits<int64_t>::max() / 8 / M) throw_invalid("timeseries too large");
+}
+
+void require(const void* p, const char* name, bool needed) {
+    if (needed && !p) throw_invalid(std::string(name) + " is NULL");
+}
+
+BandpassParams to_params(const ms3gpu_bandpass_opts* o) {
+    if (!o) throw_invalid("bandpass opts is NULL");
+    BandpassParams p;
+    p.samplerate = o->samplerate;
+    p.freq_min = o->freq_min;
+    p.freq_max = o->freq_max;
+    p.freq_wid = o->freq_wid;
+    p.quantization_unit = o->quantization_unit;
+    p.subsample_factor = o->subsample_factor ? o->subsample_factor : 1;
+    p.num_threads = o->num_threads;
+    if (p.subsample_factor < 1) throw_invalid("subsample_factor must be >= 1");
+    if (p.freq_max != 0) {
+        if (!(p.samplerate > 0)) throw_invalid("samplerate must be > 0");
+        if (p.num_threads < 1) throw_invalid("num_threads must be >= 1");
+    }
+    return p;
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+}  // namespace ms3gpu
+
+using namespace ms3gpu;
+
+extern "C" {
+
+const char* ms3gpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* ms3gpu_version(void) { return "ms3gpu 0.1.0 (sm_100a)"; }
+
+uint64_t ms3gpu_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int64_t ms3gpu_bandpass_chunk_size(int64_t M, int32_t num_threads) {
+    if (M < 1 || num_threads < 1) return -1;
+    return bandpass_chunk_size(M, num_threads);
+}
+
+int ms3gpu_bandpass_output_dims(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts, int64_t* M_out,
+                                int64_t* N_out, int32_t* dtype_out) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!opts) throw_invalid("opts is NULL");
+        const int sub = opts->subsample_factor ? opts->subsample_factor : 1;
+        if (sub < 1) throw_invalid("subsample_factor must be >= 1");
+        if (M_out) *M_out = M;
+        if (opts->freq_max == 0) {  // the input is copied unchanged
+            if (N_out) *N_out = N;
+            if (dtype_out) *dtype_out = MS3GPU_DTYPE_FLOAT32;
+            return;
+        }
+        if (N_out) *N_out = N / sub;
+        if (dtype_out) *dtype_out = opts->quantization_unit != 0 ? MS3GPU_DTYPE_INT16 : MS3GPU_DTYPE_FLOAT32;
+    });
+}
+
+int ms3gpu_bandpass_requirements(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts, double* peak_ram_mb) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!opts || !peak_ram_mb) throw_invalid("NULL argument");
+        if (opts->num_threads < 1) throw_invalid("num_threads must be >= 1");
+        // p_bandpass_filter.cpp:149-158
+        const int overhead = 6;
+        const int64_t chunk = bandpass_chunk_size(M, opts->num_threads);
+        const double bytes = overhead * sizeof(float) * (double)M * opts->num_threads * (double)(chunk + 2 * 60000);
+        *peak_ram_mb = bytes / (1024 * 1024);
+    });
+}
+
+int ms3gpu_whiten_requirements(int64_t M, int64_t N, double* peak_ram_mb) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!peak_ram_mb) throw_invalid("NULL argument");
+        // p_whiten.cpp:53-57
+        *peak_ram_mb = 3.0 * 1e5 * (double)M * sizeof(float) / (1024 * 1024);
+    });
+}
+
+int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                           const ms3gpu_bandpass_opts* opts, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        BandpassParams p = to_params(opts);
+        cudaStream_t s = as_stream(stream);
+        const bool copy = p.freq_max == 0;
+        const int64_t N2 = copy ? N : N / p.subsample_factor;
+        const size_t esz = (!copy && p.quantization_unit != 0) ? 2 : 4;
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        const size_t out_bytes = esz * (size_t)(M * N2);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(timeseries_out, "timeseries_out", out_bytes > 0);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(timeseries_out, out_bytes, s);
+        bandpass_device(static_cast<const float*>(in.ptr), M, N, out.ptr, p, s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        cudaStream_t s = as_stream(stream);
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(XXt, "XXt", M > 0);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(XXt, sizeof(double) * (size_t)(M * M), s);
+        covariance_device(static_cast<const float*>(in.ptr), M, N, static_cast<double*>(out.ptr), s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* components, double* sigma,
+                            void* stream) {
+    return guarded([&] {
+        check_shape(M, 0);
+        cudaStream_t s = as_stream(stream);
+        const size_t mm = sizeof(double) * (size_t)(M * M);
+        require(XXt, "XXt", M > 0);
+        require(W, "W", M > 0);
+        InView in;
+        stage_in(in, XXt, mm, s);
+        OutView w, c, sg;
+        w.setup(W, mm, s);
+        if (components) c.setup(components, mm, s);
+        if (sigma) sg.setup(sigma, sizeof(double) * (size_t)M, s);
+        whitening_matrix_device(static_cast<const double*>(in.ptr), M, static_cast<double*>(w.ptr),
+                                components ? static_cast<double*>(c.ptr) : nullptr,
+                                sigma ? static_cast<double*>(sg.ptr) : nullptr, s);
+        w.finish(s);
+        if (components) c.finish(s);
+        if (sigma) sg.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N, const double* W,
+                                  double quantization_unit, void* timeseries_out, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        cudaStream_t s = as_stream(stream);
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        const size_t out_bytes = (quantization_unit > 0 ? 2 : 4) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(timeseries_out, "timeseries_out", out_bytes > 0);
+        require(W, "W", M > 0);
+        InView in, w;
+        stage_in(in, timeseries, in_bytes, s);
+        stage_in(w, W, sizeof(double) * (size_t)(M * M), s);
+        OutView out;
+        out.setup(timeseries_out, out_bytes, s);
+        apply_whitening_device(static_cast<const float*>(in.ptr), M, N, static_cast<const double*>(w.ptr),
+                               quantization_unit, out.ptr, s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                  const ms3gpu_whiten_opts* opts, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!opts) throw_invalid("whiten opts is NULL");
+        cudaStream_t s = as_stream(stream);
+        const double q = opts->quantization_unit;
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        const size_t out_bytes = (q > 0 ? 2 : 4) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(timeseries_out, "timeseries_out", out_bytes > 0);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(timeseries_out, out_bytes, s);
+        DevBuf mats(sizeof(double) * (size_t)(2 * M * M), s);
+        double* XXt = mats.as<double>();
+        double* W = XXt + M * M;
+        covariance_device(static_cast<const float*>(in.ptr), M, N, XXt, s);
+        whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
+        apply_whitening_device(static_cast<const float*>(in.ptr), M, N, W, q, out.ptr, s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float* filt_out, void* pre_out,
+                           const ms3gpu_bandpass_opts* bp, const ms3gpu_whiten_opts* wh, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        BandpassParams p = to_params(bp);
+        if (!wh) throw_invalid("whiten opts is NULL");
+        if (p.subsample_factor != 1 || p.quantization_unit != 0)
+            throw_invalid("bandpass_whiten needs subsample_factor 1 and quantization_unit 0");
+        cudaStream_t s = as_stream(stream);
+        const double q = wh->quantization_unit;
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        const size_t pre_bytes = (q > 0 ? 2 : 4) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(pre_out, "pre_out", pre_bytes > 0);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView filt;
+        DevBuf filt_own;
+        float* filt_d = nullptr;
+        if (filt_out) {
+            filt.setup(filt_out, in_bytes, s);
+            filt_d = static_cast<float*>(filt.ptr);
+        } else if (in_bytes) {
+            filt_own.alloc(in_bytes, s);
+            filt_d = filt_own.as<float>();
+        }
+        bandpass_device(static_cast<const float*>(in.ptr), M, N, filt_d, p, s);
+        // The staged raw input is dead once filtered: the whitened output may reuse it.
+        OutView pre;
+        pre.setup(pre_out, pre_bytes, s, &in.own);
+        DevBuf mats(sizeof(double) * (size_t)(2 * M * M), s);
+        double* XXt = mats.as<double>();
+        double* W = XXt + M * M;
+        covariance_device(filt_d, M, N, XXt, s);
+        whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
+        apply_whitening_device(filt_d, M, N, W, q, pre.ptr, s);
+        if (filt_out) filt.finish(s);
+        pre.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+}  // extern "C"

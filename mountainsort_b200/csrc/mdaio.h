@@ -1,0 +1,43 @@
+// .mda file I/O for the ms3gpu.mp processor executable.
+//
+// Format (packages/ms3/mda/mdaio.cpp:60-203): int32 data type code, int32
+// bytes per entry, int32 number of dims (negative: the dims are int64), the
+// dims, then the data column-major.  Timeseries are read as float32 with the
+// reference's conversions (mdaReadData, mdaio.cpp:205-230); outputs are
+// written to `path.tmp` and renamed when complete (mda/diskwritemda.cpp:57-149).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ms3io {
+
+constexpr int32_t kUint8 = -2, kFloat32 = -3, kInt16 = -4, kInt32 = -5, kUint16 = -6, kFloat64 = -7,
+                  kUint32 = -8;
+
+struct MdaHeader {
+    int32_t data_type = 0;
+    int32_t bytes_per_entry = 0;
+    std::vector<int64_t> dims;
+    int64_t header_size = 0;
+    bool uses64bitdims = false;
+};
+
+int bytes_per_entry(int32_t data_type);
+
+// Parses the header of `path`; false with a message on error.
+bool read_header(const std::string& path, MdaHeader& h, std::string& err);
+
+// Reads an M x N (first two dims) timeseries converted to float32.
+bool read_timeseries_f32(const std::string& path, int64_t& M, int64_t& N, std::vector<float>& data,
+                         std::string& err);
+
+// Writes an M x N array of `data_type` (kFloat32 or kInt16) from `data`.
+bool write_timeseries(const std::string& path, int32_t data_type, int64_t M, int64_t N, const void* data,
+                      std::string& err);
+
+// Byte copy that, like QFile::copy, refuses to overwrite an existing file.
+bool copy_file(const std::string& src, const std::string& dst, std::string& err);
+
+}  // namespace ms3io

@@ -1,0 +1,287 @@
+// ms3gpu.mp -- MountainLab processor executable for ms3.bandpass_filter and
+// ms3.whiten, backed by libms3gpu (CUDA, sm_100a).
+//
+// Same command-line protocol as the reference's ms3.mp
+// (packages/ms3/mountainsort3_main.cpp:379-821):
+//   ms3gpu.mp spec [name]
+//   ms3gpu.mp requirements <name> --key=value ...
+//   ms3gpu.mp ms3.bandpass_filter --timeseries=in.mda --timeseries_out=out.mda
+//       --samplerate=.. --freq_min=.. --freq_max=.. [--freq_wid=1000]
+//       [--quantization_unit=0] [--subsample_factor=1] [--_request_num_threads=T]
+//   ms3gpu.mp ms3.whiten --timeseries=in.mda --timeseries_out=out.mda [--quantization_unit=0]
+// Exit status 0 on success, -1 (255) on failure or for an unknown processor.
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "mdaio.h"
+#include "ms3gpu.h"
+
+namespace {
+
+// CLParams (packages/ms3/common/clparams.cpp:20-77): "--name=value" or
+// "--name value"; everything else is an unnamed parameter.
+struct CLParams {
+    std::map<std::string, std::string> named;
+    std::vector<std::string> unnamed;
+    bool success = true;
+    std::string error;
+    CLParams(int argc, char** argv) {
+        for (int i = 1; i < argc; i++) {
+            std::string s = argv[i];
+            if (s.rfind("--", 0) == 0) {
+                std::string name, val;
+                const size_t eq = s.find('=');
+                if (eq != std::string::npos) {
+                    name = s.substr(2, eq - 2);
+                    val = s.substr(eq + 1);
+                } else {
+                    name = s.substr(2);
+                    if (i + 1 < argc && std::string(argv[i + 1]).rfind("--", 0) != 0) val = argv[++i];
+                }
+                if (name.empty()) {
+                    success = false;
+                    error = "Problem with parameter: " + s;
+                    return;
+                }
+                named[name] = val;
+            } else {
+                unnamed.push_back(s);
+            }
+        }
+    }
+    bool has(const std::string& k) const { return named.count(k) > 0; }
+    std::string str(const std::string& k) const {
+        auto it = named.find(k);
+        return it == named.end() ? std::string() : it->second;
+    }
+    // QVariant::toDouble(): 0 for a missing or non-numeric value
+    double num(const std::string& k, double dflt) const {
+        auto it = named.find(k);
+        if (it == named.end()) return dflt;
+        char* end = nullptr;
+        const double v = std::strtod(it->second.c_str(), &end);
+        return (end && end != it->second.c_str()) ? v : 0.0;
+    }
+};
+
+std::string exe_path() {
+    char buf[4096];
+    const ssize_t n = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+    if (n <= 0) return "ms3gpu.mp";
+    buf[n] = 0;
+    return buf;
+}
+
+std::string json_escape(const std::string& s) {
+    std::string o;
+    for (char c : s) {
+        if (c == '"' || c == '\\') o += '\\';
+        o += c;
+    }
+    return o;
+}
+
+struct Param {
+    std::string name;
+    bool optional;
+    std::string default_json;  // empty: no default
+};
+
+// ProcessorSpec::get_spec (mountainsort3_main.cpp:965-983); keys sorted as
+// QJsonObject serialises them.
+std::string processor_spec(const std::string& name, const std::string& version,
+                           const std::vector<std::string>& inputs, const std::vector<std::string>& outputs,
+                           const std::vector<Param>& params, const std::string& ind) {
+    const std::string exe = exe_path();
+    auto files = [&](const std::vector<std::string>& v) {
+        std::string o = "[\n";
+        for (size_t i = 0; i < v.size(); i++) {
+            o += ind + "        {\n" + ind + "            \"description\": \"\",\n" + ind + "            \"name\": \"" +
+                 v[i] + "\",\n" + ind + "            \"optional\": false\n" + ind + "        }";
+            o += (i + 1 < v.size()) ? ",\n" : "\n";
+        }
+        return o + ind + "    ]";
+    };
+    std::string ps = "[\n";
+    for (size_t i = 0; i < params.size(); i++) {
+        const Param& p = params[i];
+        ps += ind + "        {\n";
+        if (!p.default_json.empty()) ps += ind + "            \"default_value\": " + p.default_json + ",\n";
+        ps += ind + "            \"description\": \"\",\n" + ind + "            \"name\": \"" + p.name + "\",\n" + ind +
+              "            \"optional\": " + (p.optional ? "true" : "false") + "\n" + ind + "        }";
+        ps += (i + 1 < params.size()) ? ",\n" : "\n";
+    }
+    ps += ind + "    ]";
+    std::string o = ind + "{\n";
+    o += ind + "    \"description\": \"\",\n";
+    o += ind + "    \"exe_command\": \"" + json_escape(exe) + " " + name + " $(arguments)\",\n";
+    o += ind + "    \"inputs\": " + files(inputs) + ",\n";
+    o += ind + "    \"name\": \"" + name + "\",\n";
+    o += ind + "    \"outputs\": " + files(outputs) + ",\n";
+    o += ind + "    \"parameters\": " + ps + ",\n";
+    o += ind + "    \"requirements_command\": \"" + json_escape(exe) + " requirements " + name + " $(arguments)\",\n";
+    o += ind + "    \"version\": \"" + version + "\"\n";
+    o += ind + "}";
+    return o;
+}
+
+// Registered at mountainsort3_main.cpp:146-165 (same names, versions,
+// parameters and defaults).
+std::string spec_bandpass(const std::string& ind) {
+    return processor_spec("ms3.bandpass_filter", "0.20", {"timeseries"}, {"timeseries_out"},
+                          {{"samplerate", false, ""},
+                           {"freq_min", false, ""},
+                           {"freq_max", false, ""},
+                           {"freq_wid", true, "1000"},
+                           {"quantization_unit", true, "0"},
+                           {"subsample_factor", true, "1"}},
+                          ind);
+}
+std::string spec_whiten(const std::string& ind) {
+    return processor_spec("ms3.whiten", "0.1", {"timeseries"}, {"timeseries_out"},
+                          {{"quantization_unit", true, "0"}}, ind);
+}
+
+// T of the chunk-size formula: omp_get_max_threads() in the reference, set
+// by --_request_num_threads (mountainsort3_main.cpp:428-434); without it,
+// OpenMP's default (OMP_NUM_THREADS, else the number of hardware threads).
+int geometry_threads(const CLParams& clp) {
+    const int req = (int)clp.num("_request_num_threads", 0);
+    if (req > 0) return req;
+    const char* e = std::getenv("OMP_NUM_THREADS");
+    if (e && *e) {
+        const int v = std::atoi(e);
+        if (v > 0) return v;
+    }
+    const unsigned hc = std::thread::hardware_concurrency();
+    return hc ? (int)hc : 1;
+}
+
+ms3gpu_bandpass_opts bandpass_opts(const CLParams& clp) {
+    // mountainsort3_main.cpp:547-557
+    ms3gpu_bandpass_opts o;
+    o.samplerate = clp.num("samplerate", 0);
+    o.freq_min = clp.num("freq_min", 0);
+    o.freq_max = clp.num("freq_max", 0);
+    o.freq_wid = clp.num("freq_wid", 1000);
+    o.quantization_unit = clp.num("quantization_unit", 0);
+    o.subsample_factor = (int32_t)clp.num("subsample_factor", 1);
+    if (!o.subsample_factor) o.subsample_factor = 1;
+    o.num_threads = geometry_threads(clp);
+    return o;
+}
+
+void print_requirements(double mb) { std::printf("{\n    \"peak_ram_mb\": %.17g\n}\n", mb); }
+
+int fail(const std::string& msg) {
+    std::fprintf(stderr, "ms3gpu: %s\n", msg.c_str());
+    return -1;
+}
+
+int run_bandpass(const CLParams& clp, bool requirements_only) {
+    const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
+    ms3gpu_bandpass_opts o = bandpass_opts(clp);
+    std::string err;
+    ms3io::MdaHeader h;
+    if (o.freq_max == 0 && !requirements_only) {
+        // p_bandpass_filter.cpp:117-119
+        if (!ms3io::copy_file(in, out, err)) return fail(err);
+        return 0;
+    }
+    if (!ms3io::read_header(in, h, err)) return fail(err);
+    const int64_t M = h.dims[0];
+    const int64_t N = h.dims.size() > 1 ? h.dims[1] : 1;
+    if (requirements_only) {
+        double mb = 0;
+        if (ms3gpu_bandpass_requirements(M, N, &o, &mb) != MS3GPU_OK) {
+            std::printf("Error in processor while trying to retrieve requirements.\n");
+            return -1;
+        }
+        print_requirements(mb);
+        return 0;
+    }
+    std::vector<float> X;
+    int64_t M1 = 0, N1 = 0;
+    if (!ms3io::read_timeseries_f32(in, M1, N1, X, err)) return fail(err);
+    int64_t Mo = 0, No = 0;
+    int32_t dt = 0;
+    if (ms3gpu_bandpass_output_dims(M, N, &o, &Mo, &No, &dt) != MS3GPU_OK) return fail(ms3gpu_last_error());
+    std::vector<unsigned char> Y((size_t)(Mo * No) * (dt == MS3GPU_DTYPE_INT16 ? 2 : 4));
+    std::fprintf(stderr, "ms3gpu: bandpass %lld x %lld, chunk %lld (T=%d)\n", (long long)M, (long long)N,
+                 (long long)ms3gpu_bandpass_chunk_size(M, o.num_threads), o.num_threads);
+    if (ms3gpu_bandpass_filter(X.data(), M, N, Y.data(), &o, nullptr) != MS3GPU_OK)
+        return fail(ms3gpu_last_error());
+    if (!ms3io::write_timeseries(out, dt, Mo, No, Y.data(), err)) return fail(err);
+    return 0;
+}
+
+int run_whiten(const CLParams& clp, bool requirements_only) {
+    const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
+    ms3gpu_whiten_opts o;
+    o.quantization_unit = clp.num("quantization_unit", 0);  // mountainsort3_main.cpp:576
+    std::string err;
+    ms3io::MdaHeader h;
+    if (!ms3io::read_header(in, h, err)) return fail(err);
+    const int64_t M = h.dims[0];
+    const int64_t N = h.dims.size() > 1 ? h.dims[1] : 1;
+    if (requirements_only) {
+        double mb = 0;
+        if (ms3gpu_whiten_requirements(M, N, &mb) != MS3GPU_OK) {
+            std::printf("Error in processor while trying to retrieve requirements.\n");
+            return -1;
+        }
+        print_requirements(mb);
+        return 0;
+    }
+    std::vector<float> X;
+    int64_t M1 = 0, N1 = 0;
+    if (!ms3io::read_timeseries_f32(in, M1, N1, X, err)) return fail(err);
+    const bool i16 = o.quantization_unit > 0;
+    std::vector<unsigned char> Y((size_t)(M * N) * (i16 ? 2 : 4));
+    if (ms3gpu_whiten(X.data(), M, N, Y.data(), &o, nullptr) != MS3GPU_OK) return fail(ms3gpu_last_error());
+    if (!ms3io::write_timeseries(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    CLParams clp(argc, argv);
+    if (!clp.success) return fail(clp.error);
+    const std::string arg1 = clp.unnamed.size() > 0 ? clp.unnamed[0] : "";
+    const std::string arg2 = clp.unnamed.size() > 1 ? clp.unnamed[1] : "";
+    if (arg1 == "spec") {
+        if (arg2.empty()) {
+            std::printf("{\n    \"processors\": [\n%s,\n%s\n    ]\n}\n\n", spec_bandpass("        ").c_str(),
+                        spec_whiten("        ").c_str());
+            return 0;
+        }
+        if (arg2 == "ms3.bandpass_filter") {
+            std::printf("%s\n\n", spec_bandpass("").c_str());
+            return 0;
+        }
+        if (arg2 == "ms3.whiten") {
+            std::printf("%s\n\n", spec_whiten("").c_str());
+            return 0;
+        }
+        std::printf("{}\n");
+        return -1;
+    }
+    bool requirements_only = false;
+    std::string pname = arg1;
+    if (arg1 == "requirements") {
+        pname = arg2;
+        requirements_only = true;
+    }
+    if (pname == "ms3.bandpass_filter") return run_bandpass(clp, requirements_only);
+    if (pname == "ms3.whiten") return run_whiten(clp, requirements_only);
+    std::fprintf(stderr, "Unexpected processor name: %s\n", pname.c_str());
+    return -1;
+}

@@ -1,0 +1,430 @@
+// ms3.whiten on the GPU.
+//
+// Reference: packages/ms3/p_whiten.cpp:45-206 and packages/ms3/pca.cpp.
+//   pass 1   XXt = sum_t x_t x_t^T / (N-1)            (p_whiten.cpp:64-118)
+//   matrix   W = whitening_matrix_from_XXt(XXt)        (pca.cpp:635-651)
+//   pass 2   y_t = W^T x_t, rounded to multiples of 1e-4, optional int16
+//                                                     (p_whiten.cpp:153-206)
+//
+// Kernels:
+//   cov_partial / cov_reduce   channel covariance: 64x64 channel tiles of the
+//       upper triangle x time slices.  Products are summed in FP32 over 32
+//       timepoints (round-to-nearest FMA, unbiased) and those sums in FP64,
+//       so the result agrees with the reference's double sum of float
+//       products to ~1e-10 relative.  Partial tiles are reduced in a fixed
+//       order: repeat runs are bit-identical.
+//   pca_cluster   the reference's power iteration, FP64, one thread-block
+//       cluster: the working matrix XXtw is split by rows across the CTAs'
+//       shared memory (global memory beyond what fits); each matvec result
+//       is broadcast to every CTA through distributed shared memory, one
+//       cluster barrier per matvec.  Deflation (I-cc')X(I-cc') is applied as
+//       the equivalent symmetric rank-2 update.
+//   w_assemble    W = (C D) C^T in the reference's exact summation order.
+//   apply_gemm    y = W^T x with W rounded to float, FP32 FMA accumulation,
+//       1e-4 rounding in FP64 in the epilogue (bit-exact rounding rule).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "whiten.h"
+
+namespace cg = cooperative_groups;
+
+namespace ms3gpu {
+
+namespace {
+
+// ------------------------------------------------------------ covariance
+
+constexpr int kCT = 64;  // channel tile
+constexpr int kTT = 32;  // timepoints summed in FP32 before the FP64 add
+
+__global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, int64_t M, int64_t N, int nb,
+                                                   int64_t tslice, double* __restrict__ partials) {
+    __shared__ __align__(16) float As[kTT][kCT];
+    __shared__ __align__(16) float Bs[kTT][kCT];
+    const int pair = blockIdx.x;
+    const int npairs = gridDim.x;
+    int bi = 0, rem = pair;
+    while (rem >= nb - bi) { rem -= nb - bi; bi++; }
+    const int bj = bi + rem;
+    const int64_t t_begin = (int64_t)blockIdx.y * tslice;
+    const int64_t t_end = min(N, t_begin + tslice);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double accd[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) accd[i][j] = 0.0;
+
+    for (int64_t t0 = t_begin; t0 < t_end; t0 += kTT) {
+        for (int e = threadIdx.x; e < kTT * kCT; e += blockDim.x) {
+            const int tt = e / kCT, c = e % kCT;
+            const int64_t t = t0 + tt;
+            const int64_t ma = (int64_t)bi * kCT + c, mb = (int64_t)bj * kCT + c;
+            const bool tv = t < t_end;
+            As[tt][c] = (tv && ma < M) ? X[t * M + ma] : 0.f;
+            Bs[tt][c] = (tv && mb < M) ? X[t * M + mb] : 0.f;
+        }
+        __syncthreads();
+        float acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+#pragma unroll 8
+        for (int tt = 0; tt < kTT; tt++) {
+            const float4 a = *reinterpret_cast<const float4*>(&As[tt][ty * 4]);
+            const float4 b = *reinterpret_cast<const float4*>(&Bs[tt][tx * 4]);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) accd[i][j] += (double)acc[i][j];
+        __syncthreads();
+    }
+    double* dst = partials + ((size_t)blockIdx.y * npairs + pair) * (kCT * kCT);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) dst[(ty * 4 + i) * kCT + tx * 4 + j] = accd[i][j];
+}
+
+__global__ void cov_reduce(const double* __restrict__ partials, int S, int npairs, int nb, int64_t M,
+                           int64_t N, double* __restrict__ XXt) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)npairs * kCT * kCT) return;
+    const int pair = (int)(idx / (kCT * kCT));
+    const int e = (int)(idx % (kCT * kCT));
+    const int r = e / kCT, c = e % kCT;
+    int bi = 0, rem = pair;
+    while (rem >= nb - bi) { rem -= nb - bi; bi++; }
+    const int bj = bi + rem;
+    const int64_t i = (int64_t)bi * kCT + r, j = (int64_t)bj * kCT + c;
+    if (i >= M || j >= M) return;
+    double s = 0.0;
+    for (int k = 0; k < S; k++) s += partials[((size_t)k * npairs + pair) * (kCT * kCT) + e];
+    if (N > 1) s /= (double)(N - 1);
+    XXt[i + M * j] = s;
+    XXt[j + M * i] = s;
+}
+
+// ------------------------------------------------------------ power iteration
+
+constexpr int kPcaThreads = 512;
+
+// Sum over the block of per-thread values; every thread returns the total.
+// Fixed reduction tree: identical results in every CTA of the cluster.
+__device__ double block_sum(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int i = 0; i < nw; i++) t += red[i];
+    return t;
+}
+
+// y = X v for this CTA's rows, written into `dst` of every CTA in the cluster,
+// followed by a cluster barrier.
+__device__ void cluster_matvec(cg::cluster_group& cluster, const double* __restrict__ X, int RS, int r0,
+                               int nr, int M, const double* __restrict__ v, double* dst) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    const int CS = (int)cluster.num_blocks();
+    for (int r = w; r < nr; r += nw) {
+        const double* row = X + (size_t)r * RS;
+        double s = 0.0;
+        for (int n = l; n < M; n += 32) s += row[n] * v[n];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (int d = l; d < CS; d += 32) {
+            double* remote = cluster.map_shared_rank(dst, d);
+            remote[r0 + r] = s;
+        }
+    }
+    cluster.sync();
+}
+
+// pca_from_XXt (pca.cpp:172-195) for all M components.
+// Xg: optional global copy of the rows (when they do not fit shared memory).
+__global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restrict__ XXt, int M, int R,
+                                                            int num_iter, int rows_in_smem, double* Xg,
+                                                            double* __restrict__ comps,
+                                                            double* __restrict__ sigma) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    extern __shared__ double sm[];
+    const int RS = M + 1;  // padded row stride
+    double* vb[2];
+    vb[0] = sm;
+    vb[1] = vb[0] + M;
+    double* vinit = vb[1] + M;
+    double* red = vinit + M;
+    double* X = rows_in_smem ? (red + 32) : (Xg + (size_t)rank * R * RS);
+    const int r0 = rank * R;
+    const int nr = max(0, min(R, M - r0));
+
+    for (int idx = threadIdx.x; idx < nr * M; idx += blockDim.x) {
+        const int r = idx % nr, n = idx / nr;
+        X[(size_t)r * RS + n] = XXt[(size_t)(r0 + r) + (size_t)M * n];
+    }
+    // start vector sin(i+1), normalised (pca.cpp:546-549, 457-466)
+    for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = sin((double)(n + 1));
+    __syncthreads();
+    {
+        double part = 0.0;
+        for (int n = threadIdx.x; n < M; n += blockDim.x) part += vinit[n] * vinit[n];
+        const double nrm = sqrt(block_sum(part, red));
+        __syncthreads();
+        if (nrm != 0.0)
+            for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = vinit[n] / nrm;
+    }
+    cluster.sync();
+
+    for (int k = 0; k < M; k++) {
+        int cur = 0;
+        for (int n = threadIdx.x; n < M; n += blockDim.x) vb[0][n] = vinit[n];
+        __syncthreads();
+        double sig = 0.0;
+        for (int it = 0; it < num_iter; it++) {
+            const int nxt = cur ^ 1;
+            cluster_matvec(cluster, X, RS, r0, nr, M, vb[cur], vb[nxt]);
+            double part = 0.0;
+            for (int n = threadIdx.x; n < M; n += blockDim.x) part += vb[nxt][n] * vb[nxt][n];
+            sig = sqrt(block_sum(part, red));
+            __syncthreads();
+            if (sig != 0.0)
+                for (int n = threadIdx.x; n < M; n += blockDim.x) vb[nxt][n] = vb[nxt][n] / sig;
+            __syncthreads();
+            cur = nxt;
+        }
+        const double* v = vb[cur];
+        if (rank == 0) {
+            for (int n = threadIdx.x; n < M; n += blockDim.x) comps[(size_t)n + (size_t)M * k] = v[n];
+            if (threadIdx.x == 0) sigma[k] = sig;
+        }
+        // deflation: X <- X - v u' - u v' + (v'u) v v',  u = X v
+        double* u = vb[cur ^ 1];
+        cluster_matvec(cluster, X, RS, r0, nr, M, v, u);
+        double part = 0.0;
+        for (int n = threadIdx.x; n < M; n += blockDim.x) part += v[n] * u[n];
+        const double alpha = block_sum(part, red);
+        for (int idx = threadIdx.x; idx < nr * M; idx += blockDim.x) {
+            const int r = idx / M, n = idx % M;
+            const int m = r0 + r;
+            const double s = __dadd_rn(__dmul_rn(v[m], u[n]), __dmul_rn(u[m], v[n]));
+            const double x = __dsub_rn(X[(size_t)r * RS + n], s);
+            X[(size_t)r * RS + n] = __dadd_rn(x, __dmul_rn(alpha, __dmul_rn(v[m], v[n])));
+        }
+        cluster.sync();
+    }
+}
+
+// W = (C D) C^T, D = diag(1/sqrt(sigma)) (0 where sigma == 0), in the
+// reference's order: tmp(m,l) = C(m,l) d_l (mult_AB with a diagonal,
+// pca.cpp:220-243), W(m,n) = sum_l tmp(m,l) C(n,l) (mult_ABtrans, :319-342).
+__global__ void w_assemble(const double* __restrict__ C, const double* __restrict__ sigma, int M,
+                           double* __restrict__ W) {
+    extern __shared__ double dsh[];
+    for (int l = threadIdx.x; l < M; l += blockDim.x) {
+        const double s = sigma[l];
+        dsh[l] = (s != 0.0) ? 1.0 / sqrt(s) : 0.0;
+    }
+    __syncthreads();
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = blockIdx.y;
+    if (m >= M) return;
+    double acc = 0.0;
+    for (int l = 0; l < M; l++) {
+        const double tmp = __dmul_rn(C[(size_t)m + (size_t)M * l], dsh[l]);
+        acc = __dadd_rn(acc, __dmul_rn(tmp, C[(size_t)n + (size_t)M * l]));
+    }
+    W[(size_t)m + (size_t)M * n] = acc;
+}
+
+// ------------------------------------------------------------ apply
+
+// Wt[m1][m2] = (float) W[m1*M + m2]  (the element the reference multiplies
+// x[m2] with when it accumulates out[m1], p_whiten.cpp:174-183)
+__global__ void w_to_float(const double* __restrict__ W, int64_t MM, float* __restrict__ Wt) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MM) Wt[i] = (float)W[i];
+}
+
+// quantize(x, 1e-4) = floor(x/1e-4 + 0.5) * 1e-4 in double (p_whiten.cpp:31-41).
+// x * 1e4 differs from x / 1e-4 by at most a few ulps, so its floor is used
+// unless the value sits within 1e-6 of a rounding boundary, where the exact
+// IEEE division decides.
+__device__ __forceinline__ float quantize_1e4(float x) {
+    const double xd = (double)x;
+    double t = __dadd_rn(__dmul_rn(xd, 10000.0), 0.5);
+    double f = floor(t);
+    if (t - f < 1e-6 || f + 1.0 - t < 1e-6) {
+        t = __dadd_rn(__ddiv_rn(xd, 0.0001), 0.5);
+        f = floor(t);
+    }
+    return (float)__dmul_rn(f, 0.0001);
+}
+
+constexpr int kBM = 64, kBN = 64, kBK = 16;
+
+__global__ void __launch_bounds__(256) apply_gemm(const float* __restrict__ X, const float* __restrict__ Wt,
+                                                  int64_t M, int64_t N, double qunit, void* __restrict__ out) {
+    __shared__ __align__(16) float Xs[kBK][kBM + 4];
+    __shared__ __align__(16) float Ws[kBK][kBN + 4];
+    const int64_t t0 = (int64_t)blockIdx.x * kBM;
+    const int64_t n0 = (int64_t)blockIdx.y * kBN;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+    for (int64_t k0 = 0; k0 < M; k0 += kBK) {
+        for (int e = threadIdx.x; e < kBM * kBK; e += blockDim.x) {
+            const int r = e / kBK, kk = e % kBK;
+            const int64_t t = t0 + r, k = k0 + kk;
+            Xs[kk][r] = (t < N && k < M) ? X[t * M + k] : 0.f;
+            const int64_t n = n0 + r;
+            Ws[kk][r] = (n < M && k < M) ? Wt[n * M + k] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; kk++) {
+            const float4 a = *reinterpret_cast<const float4*>(&Xs[kk][ty * 4]);
+            const float4 b = *reinterpret_cast<const float4*>(&Ws[kk][tx * 4]);
+            const float av[4] = {a.x, a.y, a.z, a.w};
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int64_t t = t0 + ty * 4 + i;
+        if (t >= N) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t n = n0 + tx * 4 + j;
+            if (n >= M) continue;
+            const float y = quantize_1e4(acc[i][j]);
+            if (qunit > 0) {
+                // scale_for_quantization (p_whiten.cpp:445-451): (int)(y/q + 0.5)
+                // stored in a float, then written as int16 by the .mda writer.
+                const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)y, qunit), 0.5));
+                static_cast<int16_t*>(out)[t * M + n] = x86_float_to_int16((float)iv);
+            } else {
+                static_cast<float*>(out)[t * M + n] = y;
+            }
+        }
+    }
+}
+
+int num_sms() {
+    int dev = 0, n = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    MS3_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+}  // namespace
+
+void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream) {
+    if (M <= 0) return;
+    const int nb = (int)ceil_div(M, kCT);
+    const int npairs = nb * (nb + 1) / 2;
+    if (N == 0) {
+        MS3_CUDA(cudaMemsetAsync(XXt, 0, sizeof(double) * (size_t)(M * M), stream));
+        return;
+    }
+    const int64_t target = std::max<int64_t>(1, (int64_t)4 * num_sms() / npairs);
+    int64_t S = std::min<int64_t>(target, ceil_div(N, kTT));
+    int64_t tslice = ceil_div(ceil_div(N, S), kTT) * kTT;
+    S = ceil_div(N, tslice);
+    DevBuf partials((size_t)S * npairs * kCT * kCT * sizeof(double), stream);
+    cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
+    MS3_LAUNCH_CHECK();
+    const int64_t total = (int64_t)npairs * kCT * kCT;
+    cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(partials.as<double>(), (int)S, npairs, nb,
+                                                                   M, N, XXt);
+    MS3_LAUNCH_CHECK();
+}
+
+void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
+                             cudaStream_t stream) {
+    if (M <= 0) return;
+    if (M > 65535) throw_unsupported("whitening matrix for more than 65535 channels");
+    DevBuf cbuf, sbuf;
+    if (!comps) { cbuf.alloc(sizeof(double) * (size_t)(M * M), stream); comps = cbuf.as<double>(); }
+    if (!sigma) { sbuf.alloc(sizeof(double) * (size_t)M, stream); sigma = sbuf.as<double>(); }
+
+    int dev = 0, max_optin = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    MS3_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t vec_bytes = sizeof(double) * (size_t)(3 * M + 32);
+    int CS = 0, R = 0, in_smem = 0;
+    for (int cs : {8, 16}) {
+        const int r = (int)ceil_div(M, cs);
+        const size_t need = vec_bytes + sizeof(double) * (size_t)r * (size_t)(M + 1);
+        if (need <= (size_t)max_optin) { CS = cs; R = r; in_smem = 1; break; }
+    }
+    DevBuf xg;
+    if (!in_smem) {
+        CS = 16;
+        R = (int)ceil_div(M, CS);
+        xg.alloc(sizeof(double) * (size_t)CS * R * (size_t)(M + 1), stream);
+    }
+    const size_t smem = vec_bytes + (in_smem ? sizeof(double) * (size_t)R * (size_t)(M + 1) : 0);
+    MS3_CUDA(cudaFuncSetAttribute(pca_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (CS > 8) MS3_CUDA(cudaFuncSetAttribute(pca_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CS, 1, 1);
+    cfg.blockDim = dim3(kPcaThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MS3_CUDA(cudaLaunchKernelEx(&cfg, pca_cluster, XXt, (int)M, R, 10, in_smem, xg.as<double>(), comps, sigma));
+    MS3_LAUNCH_CHECK();
+    const size_t wsm = sizeof(double) * (size_t)M;
+    if (wsm > 48 * 1024)
+        MS3_CUDA(cudaFuncSetAttribute(w_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    w_assemble<<<dim3((unsigned)ceil_div(M, 128), (unsigned)M), 128, wsm, stream>>>(comps, sigma, (int)M, W);
+    MS3_LAUNCH_CHECK();
+}
+
+void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
+                            void* out, cudaStream_t stream) {
+    if (M <= 0 || N <= 0) return;
+    DevBuf wt(sizeof(float) * (size_t)(M * M), stream);
+    w_to_float<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, wt.as<float>());
+    MS3_LAUNCH_CHECK();
+    const int64_t gx = ceil_div(N, kBM);
+    const int64_t gy = ceil_div(M, kBN);
+    if (gy > 65535) throw_unsupported("too many channels for the apply kernel");
+    if (gx > 0x7fffffff) throw_unsupported("too many timepoints for the apply kernel");
+    apply_gemm<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, out);
+    MS3_LAUNCH_CHECK();
+}
+
+}  // namespace ms3gpu

@@ -1,0 +1,22 @@
+// Internal interface of the whitening stages (device pointers only).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ms3gpu {
+
+// XXt (M x M doubles, column-major) = sum_t x_t x_t^T / (N-1 if N > 1).
+void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
+
+// Power-iteration whitening matrix; comps / sigma may be null.
+void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
+                             cudaStream_t stream);
+
+// out = quantize(W^T x) per timepoint; out float32, or int16 when
+// quantization_unit > 0.
+void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W,
+                            double quantization_unit, void* out, cudaStream_t stream);
+
+}  // namespace ms3gpu

@@ -1,0 +1,87 @@
+"""The C ABI library: it loads, exports every entry point include/ms3gpu.h
+declares, and its host-only functions and argument checks behave (no GPU
+needed; nothing here launches a kernel)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from mountainsort_b200 import _lib, api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ms3gpu.h")
+
+
+def header_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"MS3GPU_API\s+[\w\s\*]+?\b(ms3gpu_\w+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    syms = header_symbols()
+    for s in ["ms3gpu_bandpass_filter", "ms3gpu_whiten", "ms3gpu_bandpass_whiten", "ms3gpu_whiten_covariance",
+              "ms3gpu_whitening_matrix", "ms3gpu_apply_whitening_matrix", "ms3gpu_last_error"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    for s in header_symbols():
+        assert hasattr(L, s), s
+    assert set(header_symbols()) == set(_lib.SIGNATURES)
+
+
+def test_version_and_geometry():
+    L = _lib.load()
+    assert b"sm_100a" in L.ms3gpu_version()
+    assert api.chunk_size(384, 16) == 120000
+    assert api.chunk_size(16, 8) == 229525
+    assert api.chunk_size(4, 16) == 579050
+    assert L.ms3gpu_bandpass_chunk_size(0, 16) == -1
+
+
+def test_output_dims():
+    L = _lib.load()
+    M, N, dt = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    o = api.bandpass_opts(30000, 300, 6000, 1000, 0, 3, 16)
+    assert L.ms3gpu_bandpass_output_dims(8, 1000, ctypes.byref(o), ctypes.byref(M), ctypes.byref(N), ctypes.byref(dt)) == 0
+    assert (M.value, N.value, dt.value) == (8, 333, _lib.DTYPE_FLOAT32)
+    o = api.bandpass_opts(30000, 300, 6000, 1000, 0.5, 1, 16)
+    L.ms3gpu_bandpass_output_dims(8, 1000, ctypes.byref(o), ctypes.byref(M), ctypes.byref(N), ctypes.byref(dt))
+    assert dt.value == _lib.DTYPE_INT16
+    o = api.bandpass_opts(30000, 300, 0, 1000, 0.5, 3, 16)  # freq_max 0: a copy
+    L.ms3gpu_bandpass_output_dims(8, 1000, ctypes.byref(o), ctypes.byref(M), ctypes.byref(N), ctypes.byref(dt))
+    assert (N.value, dt.value) == (1000, _lib.DTYPE_FLOAT32)
+
+
+def test_requirements_match_reference_model(ref32):
+    for M, T in [(32, 16), (384, 16), (4, 8)]:
+        mb = api.requirements("ms3.bandpass_filter", M, 1000, samplerate=30000, freq_min=300, freq_max=6000,
+                              num_threads=T)
+        assert mb == pytest.approx(ref32.lib().ref32_bandpass_peak_ram_mb(M, T), rel=1e-15)
+        assert api.requirements("ms3.whiten", M, 1000) == pytest.approx(ref32.lib().ref32_whiten_peak_ram_mb(M), rel=1e-15)
+
+
+@pytest.mark.parametrize("call", [
+    lambda L: L.ms3gpu_bandpass_filter(None, 4, 10, None, None, None),
+    lambda L: L.ms3gpu_bandpass_filter(None, -1, 10, None, ctypes.byref(api.bandpass_opts(30000, 300, 6000)), None),
+    lambda L: L.ms3gpu_bandpass_filter(None, 4, 10, None, ctypes.byref(api.bandpass_opts(30000, 300, 6000)), None),
+    lambda L: L.ms3gpu_bandpass_filter(None, 4, 10, None, ctypes.byref(api.bandpass_opts(0, 300, 6000)), None),
+    lambda L: L.ms3gpu_whiten(None, 4, 10, None, None, None),
+    lambda L: L.ms3gpu_bandpass_whiten(None, 4, 10, None, None, ctypes.byref(api.bandpass_opts(30000, 300, 6000, 1000, 0, 2)),
+                                       ctypes.byref(_lib.WhitenOpts(0)), None),
+])
+def test_invalid_arguments_rejected_before_device_work(call):
+    L = _lib.load()
+    assert call(L) == _lib.ERR_INVALID
+    assert _lib.last_error()
+
+
+def test_bad_num_threads_rejected():
+    L = _lib.load()
+    o = api.bandpass_opts(30000, 300, 6000, 1000, 0, 1, 16)
+    o.num_threads = 0
+    buf = (ctypes.c_float * 40)()
+    assert L.ms3gpu_bandpass_filter(buf, 4, 10, buf, ctypes.byref(o), None) == _lib.ERR_INVALID
+    assert "num_threads" in _lib.last_error()

@@ -1,0 +1,89 @@
+"""The ms3gpu.mp processor executable: the MountainLab protocol surface that
+needs no GPU (spec, requirements, unknown names, argument parsing)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from mountainsort_b200 import mdaio
+
+EXE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "mountainsort_b200", "ms3gpu.mp")
+
+
+def run(*args, env=None):
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    return subprocess.run([EXE, *args], capture_output=True, text=True, env=e, timeout=60)
+
+
+def test_spec_lists_the_two_processors():
+    r = run("spec")
+    assert r.returncode == 0
+    spec = json.loads(r.stdout)
+    by = {p["name"]: p for p in spec["processors"]}
+    assert set(by) == {"ms3.bandpass_filter", "ms3.whiten"}
+    bp = by["ms3.bandpass_filter"]
+    assert bp["version"] == "0.20"
+    params = {p["name"]: p for p in bp["parameters"]}
+    assert [n for n in params if not params[n]["optional"]] == ["samplerate", "freq_min", "freq_max"]
+    assert params["freq_wid"]["default_value"] == 1000
+    assert params["quantization_unit"]["default_value"] == 0
+    assert params["subsample_factor"]["default_value"] == 1
+    assert bp["inputs"][0]["name"] == "timeseries" and bp["outputs"][0]["name"] == "timeseries_out"
+    assert bp["exe_command"].endswith("ms3.bandpass_filter $(arguments)")
+    assert bp["requirements_command"].endswith("requirements ms3.bandpass_filter $(arguments)")
+    assert by["ms3.whiten"]["version"] == "0.1"
+
+
+def test_spec_single_and_unknown():
+    r = run("spec", "ms3.whiten")
+    assert r.returncode == 0 and json.loads(r.stdout)["name"] == "ms3.whiten"
+    r = run("spec", "ms3.nope")
+    assert r.returncode == 255 and r.stdout.strip() == "{}"
+    assert run("ms3.nope").returncode == 255
+
+
+def test_requirements(tmp_path, ref32):
+    p = str(tmp_path / "raw.mda")
+    mdaio.writemda(np.zeros((32, 100), np.float32), p)
+    r = run("requirements", "ms3.bandpass_filter", f"--timeseries={p}", "--timeseries_out=x.mda",
+            "--samplerate=30000", "--freq_min=300", "--freq_max=6000", "--_request_num_threads=16")
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout)["peak_ram_mb"] == pytest.approx(ref32.lib().ref32_bandpass_peak_ram_mb(32, 16))
+    # without _request_num_threads, T comes from OMP_NUM_THREADS like omp_get_max_threads()
+    r = run("requirements", "ms3.bandpass_filter", "--timeseries", p, "--samplerate", "30000", "--freq_min=300",
+            "--freq_max=6000", env={"OMP_NUM_THREADS": "4"})
+    assert json.loads(r.stdout)["peak_ram_mb"] == pytest.approx(ref32.lib().ref32_bandpass_peak_ram_mb(32, 4))
+    r = run("requirements", "ms3.whiten", f"--timeseries={p}", "--timeseries_out=y.mda")
+    assert json.loads(r.stdout)["peak_ram_mb"] == pytest.approx(ref32.lib().ref32_whiten_peak_ram_mb(32))
+
+
+def test_missing_or_corrupt_input_fails_without_output(tmp_path):
+    out = str(tmp_path / "o.mda")
+    r = run("ms3.whiten", f"--timeseries={tmp_path / 'missing.mda'}", f"--timeseries_out={out}")
+    assert r.returncode == 255 and not os.path.exists(out)
+    bad = tmp_path / "bad.mda"
+    bad.write_bytes(b"\x00\x01")
+    r = run("ms3.bandpass_filter", f"--timeseries={bad}", f"--timeseries_out={out}", "--samplerate=30000",
+            "--freq_min=300", "--freq_max=6000")
+    assert r.returncode == 255 and not os.path.exists(out)
+    d = tmp_path / "dir_input"
+    d.mkdir()
+    r = run("ms3.whiten", f"--timeseries={d}", f"--timeseries_out={out}")
+    assert r.returncode == 255 and "directory" in r.stderr
+
+
+def test_freq_max_zero_copies_file(tmp_path):
+    src = str(tmp_path / "raw.mda")
+    mdaio.writemda(np.arange(12, dtype=np.float32).reshape(3, 4), src)
+    out = str(tmp_path / "o.mda")
+    r = run("ms3.bandpass_filter", f"--timeseries={src}", f"--timeseries_out={out}", "--samplerate=30000",
+            "--freq_min=300", "--freq_max=0")
+    assert r.returncode == 0
+    assert open(out, "rb").read() == open(src, "rb").read()
+    # QFile::copy semantics: an existing destination is not overwritten
+    r = run("ms3.bandpass_filter", f"--timeseries={src}", f"--timeseries_out={out}", "--freq_max=0")
+    assert r.returncode == 255

@@ -1,0 +1,199 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Gates (written in each test):
+  * filtered output vs ref32: relative L2 <= 1e-5 (plain FP32 form);
+  * whitened output vs ref32: relative L2 <= 1e-5 (it is rounded to 1e-4, so
+    differences are whole rounding steps at rounding boundaries);
+  * covariance and whitening matrix vs the oracle: relative <= 1e-8 / 1e-10;
+  * int16 outputs: identical except at truncation boundaries.
+"""
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from mountainsort_b200 import _lib, api, mdaio, synth
+from oracle import oracle64 as o64
+
+pytestmark = pytest.mark.gpu
+
+FS, FMIN, FMAX, FWID = 30000.0, 300.0, 6000.0, 1000.0
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def rel(a, b):
+    return o64.rel_l2(a, b)
+
+
+@pytest.fixture(scope="module")
+def rec32():
+    return synth.generate_numpy(32, 360000, K=12, seed=0, sites=(3, 6))
+
+
+# (M, N, T): T chosen to exercise the canonical L = 240000 and odd windows
+BP_CASES = [
+    (32, 360000, 16),   # L = 240000, 3 whole chunks
+    (12, 250000, 16),   # L = 240000, last chunk partial
+    (7, 1000, 27),      # N shorter than one chunk, odd M (last pair padded)
+    (1, 5000, 187),     # a single channel
+    (3, 130000, 63),    # odd M
+    (4, 150000, 16),    # L = 699050 = 2*5^2*11*31*41: generic radices
+    (64, 240000, 16),   # 2 groups of 16 channel pairs
+]
+
+
+@pytest.mark.parametrize("M,N,T", BP_CASES)
+def test_bandpass_parity(gpu_lib, ref32, M, N, T):
+    X = synth.generate_numpy(M, N, K=max(1, M // 3), seed=M + N, sites=(1, min(M, 4)))
+    ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=T)
+    got = api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=T)
+    assert got.shape == ref.shape and got.dtype == np.float32
+    assert rel(got, ref) <= 1e-5  # gate: plain FP32 form
+    assert rel(got, ref) <= 2e-6  # what accurate FP32 FFTs give
+
+
+def test_bandpass_device_pointers_and_determinism(gpu_lib, rec32):
+    import torch
+
+    Xd = torch.from_numpy(rec32).cuda()
+    a = api.bandpass_filter(Xd, FS, FMIN, FMAX, FWID, num_threads=16)
+    b = api.bandpass_filter(Xd, FS, FMIN, FMAX, FWID, num_threads=16)
+    h = api.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
+    assert a.is_cuda
+    assert torch.equal(a, b)
+    np.testing.assert_array_equal(a.cpu().numpy(), h)
+
+
+def test_bandpass_no_lowcut(gpu_lib, ref32):
+    X = synth.generate_numpy(16, 200000, K=3, seed=11)
+    ref = ref32.bandpass_filter(X, FS, 0.0, FMAX, FWID, num_threads=16)
+    got = api.bandpass_filter(X, FS, 0.0, FMAX, FWID, num_threads=16)
+    assert rel(got, ref) <= 1e-5
+
+
+@pytest.mark.parametrize("q", [0.5, 2.0])
+def test_bandpass_int16(gpu_lib, ref32, rec32, q):
+    ref = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, quantization_unit=q, num_threads=16)
+    got = api.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, quantization_unit=q, num_threads=16)
+    assert got.dtype == np.int16 and got.shape == ref.shape
+    d = np.abs(got.astype(np.int32) - ref.astype(np.int32))
+    assert d.max() <= 1  # truncation boundaries only
+    assert np.mean(d) < 1e-4
+
+
+@pytest.mark.parametrize("sub", [3, 7])
+def test_bandpass_subsample(gpu_lib, ref32, sub):
+    X = synth.generate_numpy(10, 250000, K=3, seed=5)
+    ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, subsample_factor=sub, num_threads=19)
+    got = api.bandpass_filter(X, FS, FMIN, FMAX, FWID, subsample_factor=sub, num_threads=19)
+    assert got.shape == ref.shape
+    assert rel(got, ref) <= 1e-5
+
+
+def test_bandpass_copy_when_freq_max_zero(gpu_lib, rec32):
+    got = api.bandpass_filter(rec32[:1000], FS, FMIN, 0.0, FWID, num_threads=16)
+    np.testing.assert_array_equal(got, rec32[:1000])
+
+
+@pytest.mark.parametrize("M", [8, 32, 64, 100])
+def test_whiten_stages_parity(gpu_lib, ref32, M):
+    X = synth.generate_numpy(M, 120000, K=M // 2, seed=M)
+    F = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=max(16, 187 // M + 1))
+    C_ref = ref32.whiten_xxt(F)
+    C = api.whiten_covariance(F)
+    assert rel(C, C_ref) <= 1e-8
+    np.testing.assert_array_equal(C, C.T)
+    W_ref, comps_ref, sig_ref = ref32.whitening_matrix(C_ref)
+    W, comps, sig = api.whitening_matrix(C_ref, return_components=True)
+    assert rel(W, W_ref) <= 1e-10
+    assert rel(sig, sig_ref) <= 1e-10
+    pre_ref, _, _ = ref32.whiten(F)
+    pre = api.whiten(F)
+    assert rel(pre, pre_ref) <= 1e-5  # gate
+    # values are multiples of 1e-4 like the reference's
+    assert np.max(np.abs(pre.astype(np.float64) * 1e4 - np.round(pre.astype(np.float64) * 1e4))) < 1e-2
+
+
+@pytest.mark.parametrize("M", [500, 700])
+def test_whitening_matrix_large_m(gpu_lib, M):
+    # 500: rows in a 16-CTA cluster's shared memory; 700: rows in global memory
+    rng = np.random.default_rng(M)
+    A = np.eye(M) + 0.3 * rng.standard_normal((M, M)) / np.sqrt(M)
+    C = A @ A.T * 37.0
+    W64, _, sig64 = o64.whitening_matrix(C)
+    W, comps, sig = api.whitening_matrix(C, return_components=True)
+    assert rel(W, W64) <= 1e-10
+    assert rel(sig, sig64) <= 1e-10
+
+
+def test_whiten_int16(gpu_lib, ref32, rec32):
+    F = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
+    ref, _, _ = ref32.whiten(F, quantization_unit=0.01)
+    got = api.whiten(F, quantization_unit=0.01)
+    assert got.dtype == np.int16
+    d = np.abs(got.astype(np.int32) - ref.astype(np.int32))
+    assert d.max() <= 1 and np.mean(d) < 1e-3
+
+
+def test_fused_pipeline_config1_geometry(gpu_lib, ref32, rec32):
+    """ms3.bandpass_filter then ms3.whiten, as mountainsort3.mlp runs them."""
+    filt_ref = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre_ref, _, _ = ref32.whiten(filt_ref)
+    filt, pre = api.bandpass_whiten(rec32, FS, FMIN, FMAX, FWID, num_threads=16, want_filt=True)
+    assert rel(filt, filt_ref) <= 1e-5
+    assert rel(pre, pre_ref) <= 1e-5
+    pre_only = api.bandpass_whiten(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
+    np.testing.assert_array_equal(pre_only, pre)
+    # against the FP64 oracle too (the floor of the FP32 forms)
+    y, q64, _, _ = o64.whiten(o64.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16))
+    assert rel(pre, q64) <= 1e-4
+
+
+def test_unsupported_window_is_a_clean_error(gpu_lib):
+    # M=6, T=16 -> L = 466033 (prime): not handled by the GPU factorisation
+    X = np.zeros((1000, 6), np.float32)
+    with pytest.raises(_lib.Ms3GpuError) as e:
+        api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    assert e.value.code == _lib.ERR_UNSUPPORTED
+    # the context stays usable
+    api.bandpass_filter(np.zeros((1000, 6), np.float32), FS, FMIN, FMAX, FWID, num_threads=32)
+
+
+def test_out_of_memory_hook_reports_nomem(gpu_lib):
+    code = (
+        "import numpy as np, sys; sys.path.insert(0, %r)\n"
+        "from mountainsort_b200 import api, _lib\n"
+        "try:\n"
+        "    api.whiten(np.ones((1000, 4), np.float32))\n"
+        "    print('NOERR')\n"
+        "except _lib.Ms3GpuError as e:\n"
+        "    print('CODE', e.code)\n"
+        "api_ok = True\n" % ROOT)
+    env = dict(os.environ, MS3GPU_FAIL_ALLOC_AFTER="0")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert "CODE %d" % _lib.ERR_NOMEM in r.stdout, r.stdout + r.stderr
+
+
+def test_processor_executable_end_to_end(gpu_lib, ref32, tmp_path):
+    X = synth.generate_numpy(16, 200000, K=4, seed=21)
+    raw = str(tmp_path / "raw.mda")
+    mdaio.writemda(X.T, raw)  # M x N column-major
+    filt, pre = str(tmp_path / "filt.mda"), str(tmp_path / "pre.mda")
+    exe = os.path.join(ROOT, "mountainsort_b200", "ms3gpu.mp")
+    r = subprocess.run([exe, "ms3.bandpass_filter", f"--timeseries={raw}", f"--timeseries_out={filt}",
+                        "--samplerate=30000", "--freq_min=300", "--freq_max=6000", "--_request_num_threads=16"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe, "ms3.whiten", f"--timeseries={filt}", f"--timeseries_out={pre}"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    F = mdaio.readmda(filt)
+    P = mdaio.readmda(pre)
+    assert F.shape == (16, 200000) and F.dtype == np.float32
+    filt_ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre_ref, _, _ = ref32.whiten(filt_ref)
+    assert rel(F.T, filt_ref) <= 1e-5
+    assert rel(P.T, pre_ref) <= 1e-5
