@@ -39,7 +39,7 @@ SIZES = {
     # name: (M, N, units, description)
     "c2": (384, 18_000_000, 300, "384ch x 18M timepoints (10 min @ 30 kHz), config 2"),
     "c1": (32, 1_800_000, 20, "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1"),
-    "small": (384, 1_200_000, 20, "384ch x 1.2M timepoints (40 s @ 30 kHz), profiling case"),
+    "small": (384, 600_000, 20, "384ch x 600k timepoints (20 s @ 30 kHz), profiling case"),
 }
 
 
@@ -158,7 +158,7 @@ def run_reference_arm(args, size):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    threads = min(threads, int(os.environ.get("MS3_BENCH_CPU_THREADS", "32")))
+    threads = min(threads, int(os.environ.get("MS3_BENCH_CPU_THREADS", "16")))
     vals = []
     for i in range(args.warmup + args.steps):
         cb = cpu_baseline(M, N, threads)
@@ -334,7 +334,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = min(os.cpu_count() or 1, int(os.environ.get("MS3_BENCH_CPU_THREADS", "32")))
+        threads = min(os.cpu_count() or 1, int(os.environ.get("MS3_BENCH_CPU_THREADS", "16")))
         cpu = cpu_baseline(M, N, threads)
 
     if rank == 0:

@@ -428,7 +428,8 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     g.N = N;
     g.paired = plan->paired;
     g.P = g.paired ? (M + 1) / 2 : M;
-    g.m_even = (M % 2 == 0);
+    // float2 loads/stores need even M and 8-byte aligned caller buffers
+    g.m_even = (M % 2 == 0) && ((uintptr_t)raw % 8 == 0) && ((uintptr_t)out % 8 == 0);
     g.L = L;
     g.L1 = plan->L1;
     g.L2 = plan->L2;

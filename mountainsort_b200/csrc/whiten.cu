@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "whiten.h"
@@ -377,7 +378,12 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
     MS3_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t vec_bytes = sizeof(double) * (size_t)(3 * M + 32);
     int CS = 0, R = 0, in_smem = 0;
+    // MS3GPU_PCA_ROWS_GLOBAL=1 keeps the working matrix in global memory
+    // even when it fits shared memory (exercises that path in tests).
+    const char* force_global = std::getenv("MS3GPU_PCA_ROWS_GLOBAL");
+    const bool allow_smem = !(force_global && force_global[0] == '1');
     for (int cs : {8, 16}) {
+        if (!allow_smem) break;
         const int r = (int)ceil_div(M, cs);
         const size_t need = vec_bytes + sizeof(double) * (size_t)r * (size_t)(M + 1);
         if (need <= (size_t)max_optin) { CS = cs; R = r; in_smem = 1; break; }
