@@ -40,6 +40,7 @@
 #include "bandpass.h"
 #include "common.cuh"
 #include "fft_block.cuh"
+#include "fft_reg.cuh"
 
 namespace ms3gpu {
 
@@ -76,6 +77,21 @@ __device__ __forceinline__ float2 load_signal(const float* __restrict__ raw, con
     return make_float2(row[m0], (m0 + 1 < g.M) ? row[m0 + 1] : 0.f);
 }
 
+// Units are ordered group-major: consecutive units are consecutive windows of
+// the same channel group, so the half of a window shared with the previous
+// window is read again while it is still in L2.
+struct UnitIdx {
+    int64_t c;
+    int grp;
+};
+__device__ __forceinline__ UnitIdx unit_index(const Geom& g, int64_t unit) {
+    const int64_t nchunks = (g.N + g.chunk - 1) / g.chunk;
+    UnitIdx u;
+    u.grp = (int)(unit / nchunks);
+    u.c = unit % nchunks;
+    return u;
+}
+
 __device__ __forceinline__ void load_plan(SubFft& dst, const SubFft& src) {
     int* d = reinterpret_cast<int*>(&dst);
     const int* s = reinterpret_cast<const int*>(&src);
@@ -99,9 +115,9 @@ __global__ void __launch_bounds__(kThreads) bp_cols_forward(const float* __restr
     for (int i = threadIdx.x; i < P1.twlen; i += blockDim.x) twS[i] = tw1[i];
 
     const int n2 = blockIdx.x;
-    const int64_t unit = unit0 + blockIdx.y;
-    const int64_t c = unit / g.ngroups;
-    const int grp = (int)(unit % g.ngroups);
+    const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
+    const int64_t c = ui.c;
+    const int grp = ui.grp;
     const int64_t t0 = c * g.chunk - kOverlap + n2;
     for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
         const int n1 = idx >> g.log2G;
@@ -179,9 +195,9 @@ __global__ void __launch_bounds__(kThreads) bp_cols_inverse(const float2* __rest
     for (int i = threadIdx.x; i < P1.twlen; i += blockDim.x) twS[i] = tw1[i];
 
     const int n2 = blockIdx.x;
-    const int64_t unit = unit0 + blockIdx.y;
-    const int64_t c = unit / g.ngroups;
-    const int grp = (int)(unit % g.ngroups);
+    const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
+    const int64_t c = ui.c;
+    const int grp = ui.grp;
     const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
     for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
         const int k1 = idx >> g.log2G;
@@ -223,6 +239,223 @@ __global__ void __launch_bounds__(kThreads) bp_cols_inverse(const float2* __rest
         }
     }
 }
+
+
+// Stores one filtered complex sample (two channels) at window index n of
+// window c, applying the trim to [60000, 60000 + chunk), the subsampling and
+// the int16 quantization of the reference (p_bandpass_filter.cpp:196-212).
+__device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geom& g, int64_t c, int64_t s,
+                                               int64_t n, float2 v) {
+    if (s >= g.P) return;
+    const int64_t j = n - kOverlap;
+    if (j < 0 || j >= g.chunk) return;
+    if (g.sub != 1 && (j % g.sub)) return;
+    const int64_t jj = j / g.sub;
+    if (jj >= g.chunk / g.sub) return;
+    const int64_t ot = (c * g.chunk) / g.sub + jj;
+    if (ot >= g.N2) return;
+    const int64_t m0 = g.paired ? 2 * s : s;
+    const bool has2 = g.paired && (m0 + 1 < g.M);
+    const size_t o = (size_t)(ot * g.M + m0);
+    if (g.out_i16) {
+        int16_t* o16 = static_cast<int16_t*>(out);
+        o16[o] = x86_float_to_int16((float)((double)v.x * g.qscale));
+        if (has2) o16[o + 1] = x86_float_to_int16((float)((double)v.y * g.qscale));
+    } else {
+        float* of = static_cast<float*>(out);
+        if (has2 && g.m_even) {
+            *reinterpret_cast<float2*>(of + o) = v;
+        } else {
+            of[o] = v.x;
+            if (has2) of[o + 1] = v.y;
+        }
+    }
+}
+
+// ------------------------------------------------- register-pass kernels
+// Each sub-transform of length n = RA * RB runs as two Stockham passes whose
+// butterflies live entirely in registers (RegDft), with one shared-memory
+// exchange between them:
+//   pass 1 (radix RA, p = 1):  item i < RB reads x[i + q RB], writes y[i RA + q]
+//   pass 2 (radix RB, p = RA): item i < RA reads y[i + q RA] * w_n^{q i},
+//                              writes z[i + q RA]   (natural order)
+// Global loads feed pass 1 directly and pass 2 stores directly.
+
+// F1, forward columns of length L1 = RA * RB.
+template <int RA, int RB>
+__global__ void __launch_bounds__(256) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
+                                                        Geom g, const float2* __restrict__ roots, int64_t unit0) {
+    constexpr int n = RA * RB;
+    extern __shared__ float4 smem_f4[];
+    float2* buf = reinterpret_cast<float2*>(smem_f4);
+    float2* rt = buf + ((size_t)n << g.log2G);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
+    const int G = 1 << g.log2G;
+    const int n2 = blockIdx.x;
+    const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
+    const int64_t t0 = ui.c * g.chunk - kOverlap + n2;
+    const int64_t s0 = (int64_t)ui.grp * G;
+    for (int it = threadIdx.x; it < (RB << g.log2G); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> g.log2G;
+        float2 u[RA];
+#pragma unroll
+        for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * g.L2, s0 + gi);
+        RegDft<RA, false>::run(u);
+#pragma unroll
+        for (int q = 0; q < RA; q++) buf[((i * RA + q) << g.log2G) + gi] = u[q];
+    }
+    __syncthreads();
+    float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
+    for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> g.log2G;
+        float2 u[RB];
+#pragma unroll
+        for (int q = 0; q < RB; q++) {
+            const float2 v = buf[((i + q * RA) << g.log2G) + gi];
+            u[q] = (q == 0) ? v : cmul(v, rt[q * i]);
+        }
+        RegDft<RB, false>::run(u);
+#pragma unroll
+        for (int q = 0; q < RB; q++) slab[(((size_t)(i + q * RA) * g.L2 + n2) << g.log2G) + gi] = u[q];
+    }
+}
+
+// F2, one k1 row: twiddle, forward L2 = SA * SB, band kernel, inverse, twiddle.
+// The forward pass 2 and the inverse pass 1 (radix SB, p = 1) share the same
+// item -> thread mapping, so the spectrum never leaves registers between them.
+// Launched with exactly SA * G threads (one middle-phase item per thread).
+template <int SA, int SB>
+__global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scratch, Geom g,
+                                                       const float2* __restrict__ roots,
+                                                       const float2* __restrict__ twL,
+                                                       const float* __restrict__ kern) {
+    constexpr int n = SA * SB;
+    extern __shared__ float4 smem_f4[];
+    float2* buf = reinterpret_cast<float2*>(smem_f4);
+    float2* rt = buf + ((size_t)n << g.log2G);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
+    const int G = 1 << g.log2G;
+    const int k1 = blockIdx.x;
+    float2* row = scratch + (size_t)blockIdx.y * (size_t)(g.L * G) + (((size_t)k1 * g.L2) << g.log2G);
+    const float2* twrow = twL + (size_t)k1 * g.L2;
+    const float* krow = kern + (size_t)k1 * g.L2;
+    // forward pass 1 (radix SA over items i < SB)
+    for (int it = threadIdx.x; it < (SB << g.log2G); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> g.log2G;
+        float2 u[SA];
+#pragma unroll
+        for (int q = 0; q < SA; q++) {
+            const int n2 = i + q * SB;
+            u[q] = cmul(row[(n2 << g.log2G) + gi], __ldg(&twrow[n2]));
+        }
+        RegDft<SA, false>::run(u);
+#pragma unroll
+        for (int q = 0; q < SA; q++) buf[((i * SA + q) << g.log2G) + gi] = u[q];
+    }
+    __syncthreads();
+    // forward pass 2 (radix SB, item i < SA), kernel, inverse pass 1 (radix SB)
+    const int it = threadIdx.x;
+    const bool active = it < (SA << g.log2G);
+    const int gi = it & (G - 1), i = it >> g.log2G;
+    float2 u[SB];
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < SB; q++) {
+            const float2 v = buf[((i + q * SA) << g.log2G) + gi];
+            u[q] = (q == 0) ? v : cmul(v, rt[q * i]);
+        }
+        RegDft<SB, false>::run(u);
+#pragma unroll
+        for (int q = 0; q < SB; q++) {
+            const float kv = __ldg(&krow[i + q * SA]);
+            u[q] = make_float2(u[q].x * kv, u[q].y * kv);
+        }
+        RegDft<SB, true>::run(u);
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < SB; q++) buf[((i * SB + q) << g.log2G) + gi] = u[q];
+    }
+    __syncthreads();
+    // inverse pass 2 (radix SA, p = SB, items i < SB)
+    for (int it2 = threadIdx.x; it2 < (SB << g.log2G); it2 += blockDim.x) {
+        const int gj = it2 & (G - 1), j = it2 >> g.log2G;
+        float2 v[SA];
+#pragma unroll
+        for (int q = 0; q < SA; q++) {
+            const float2 x = buf[((j + q * SB) << g.log2G) + gj];
+            if (q == 0) {
+                v[q] = x;
+            } else {
+                float2 w = rt[q * j];
+                w.y = -w.y;
+                v[q] = cmul(x, w);
+            }
+        }
+        RegDft<SA, true>::run(v);
+#pragma unroll
+        for (int q = 0; q < SA; q++) {
+            const int n2 = j + q * SB;
+            float2 w = __ldg(&twrow[n2]);
+            w.y = -w.y;
+            row[(n2 << g.log2G) + gj] = cmul(v[q], w);
+        }
+    }
+}
+
+// F3, inverse columns of length L1 = RA * RB (inverse order: radix RB, then
+// radix RA), trim / subsample / quantize, store.
+template <int RA, int RB>
+__global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict__ scratch, void* __restrict__ out,
+                                                        Geom g, const float2* __restrict__ roots, int64_t unit0) {
+    constexpr int n = RA * RB;
+    extern __shared__ float4 smem_f4[];
+    float2* buf = reinterpret_cast<float2*>(smem_f4);
+    float2* rt = buf + ((size_t)n << g.log2G);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
+    const int G = 1 << g.log2G;
+    const int n2 = blockIdx.x;
+    const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
+    const int64_t s0 = (int64_t)ui.grp * G;
+    const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
+    for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> g.log2G;
+        float2 u[RB];
+#pragma unroll
+        for (int q = 0; q < RB; q++) u[q] = slab[(((size_t)(i + q * RA) * g.L2 + n2) << g.log2G) + gi];
+        RegDft<RB, true>::run(u);
+#pragma unroll
+        for (int q = 0; q < RB; q++) buf[((i * RB + q) << g.log2G) + gi] = u[q];
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < (RB << g.log2G); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> g.log2G;
+        float2 u[RA];
+#pragma unroll
+        for (int q = 0; q < RA; q++) {
+            const float2 x = buf[((i + q * RB) << g.log2G) + gi];
+            if (q == 0) {
+                u[q] = x;
+            } else {
+                float2 w = rt[q * i];
+                w.y = -w.y;
+                u[q] = cmul(x, w);
+            }
+        }
+        RegDft<RA, true>::run(u);
+#pragma unroll
+        for (int q = 0; q < RA; q++) {
+            const int64_t n1 = i + q * RB;
+            store_filtered(out, g, ui.c, s0 + gi, n1 * g.L2 + n2, u[q]);
+        }
+    }
+}
+
+// Two-pass factorisations compiled for the reference's canonical window
+// (chunk 120000, L = 240000 = 480 x 500, used whenever M * T >= 187).
+constexpr int kFastRA = 16, kFastRB = 30;  // L1 = 480
+constexpr int kFastSA = 20, kFastSB = 25;  // L2 = 500
 
 // ---------------------------------------------------------------- plans
 
@@ -282,6 +515,9 @@ struct BandpassPlan {
     float2* tw2 = nullptr;  // P2 twiddles
     float2* twL = nullptr;  // [k1][n2] exp(-2 pi i n2 k1 / L)
     float* kern = nullptr;  // [k1][k2] kernel[k1 + L1 k2] / L
+    float2* root1 = nullptr;  // exp(-2 pi i e / L1), e < L1
+    float2* root2 = nullptr;  // exp(-2 pi i e / L2), e < L2
+    bool fast = false;        // L1 x L2 = 480 x 500: register-pass kernels
     ~BandpassPlan() {
         int cur = -1;
         cudaGetDevice(&cur);
@@ -290,6 +526,8 @@ struct BandpassPlan {
         cudaFree(tw2);
         cudaFree(twL);
         cudaFree(kern);
+        cudaFree(root1);
+        cudaFree(root2);
         if (cur >= 0) cudaSetDevice(cur);
     }
 };
@@ -365,6 +603,22 @@ std::shared_ptr<BandpassPlan> build_plan(int64_t L, double fs, double fmin, doub
     if (!tw2.empty()) MS3_CUDA(cudaMemcpy(plan->tw2, tw2.data(), tw2.size() * sizeof(float2), cudaMemcpyHostToDevice));
     MS3_CUDA(cudaMemcpy(plan->twL, twL.data(), (size_t)L * sizeof(float2), cudaMemcpyHostToDevice));
     MS3_CUDA(cudaMemcpy(plan->kern, kern.data(), (size_t)L * sizeof(float), cudaMemcpyHostToDevice));
+    auto roots = [](int64_t n) {
+        std::vector<float2> r((size_t)n);
+        for (int64_t e = 0; e < n; e++) {
+            const double a = -2.0 * M_PI * (double)e / (double)n;
+            r[(size_t)e] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        return r;
+    };
+    const std::vector<float2> r1 = roots(L1), r2 = roots(L2);
+    MS3_CUDA(cudaMalloc(&plan->root1, (size_t)L1 * sizeof(float2)));
+    MS3_CUDA(cudaMalloc(&plan->root2, (size_t)L2 * sizeof(float2)));
+    MS3_CUDA(cudaMemcpy(plan->root1, r1.data(), (size_t)L1 * sizeof(float2), cudaMemcpyHostToDevice));
+    MS3_CUDA(cudaMemcpy(plan->root2, r2.data(), (size_t)L2 * sizeof(float2), cudaMemcpyHostToDevice));
+    plan->fast = plan->paired && L1 == kFastRA * kFastRB && L2 == kFastSA * kFastSB;
+    const char* nofast = std::getenv("MS3GPU_BP_GENERIC");
+    if (nofast && nofast[0] == '1') plan->fast = false;
     return plan;
 }
 
@@ -463,9 +717,16 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
         int dev = 0;
         MS3_CUDA(cudaGetDevice(&dev));
         if (dev < 64 && !attrs_set[dev]) {
-            MS3_CUDA(cudaFuncSetAttribute(bp_cols_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-            MS3_CUDA(cudaFuncSetAttribute(bp_rows_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
-            MS3_CUDA(cudaFuncSetAttribute(bp_cols_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget));
+            const int lim = (int)kSmemBudget;
+            MS3_CUDA(cudaFuncSetAttribute(bp_cols_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bp_rows_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bp_cols_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_forward<kFastRA, kFastRB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_rows_filter<kFastSA, kFastSB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_inverse<kFastRA, kFastRB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             attrs_set[dev] = true;
         }
     }
@@ -475,17 +736,29 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
         MS3_CUDA(cudaMemsetAsync(out, 0, esz * (size_t)(M * N2), stream));
     }
     DevBuf scratch((size_t)per_batch * unit_bytes, stream);
+    const size_t fsm1 = ((size_t)plan->L1 * G + plan->L1) * sizeof(float2);
+    const size_t fsm2 = ((size_t)plan->L2 * G + plan->L2) * sizeof(float2);
     for (int64_t u0 = 0; u0 < units; u0 += per_batch) {
         const int64_t nb = std::min<int64_t>(per_batch, units - u0);
         dim3 g1((unsigned)plan->L2, (unsigned)nb);
         dim3 g2((unsigned)plan->L1, (unsigned)nb);
-        bp_cols_forward<<<g1, kThreads, sm1, stream>>>(raw, scratch.as<float2>(), g, plan->P1, plan->tw1, u0);
-        MS3_LAUNCH_CHECK();
-        bp_rows_filter<<<g2, kThreads, sm2, stream>>>(scratch.as<float2>(), g, plan->P2, plan->tw2, plan->twL,
-                                                     plan->kern);
-        MS3_LAUNCH_CHECK();
-        bp_cols_inverse<<<g1, kThreads, sm1, stream>>>(scratch.as<float2>(), out, g, plan->P1, plan->tw1, u0);
-        MS3_LAUNCH_CHECK();
+        float2* sc = scratch.as<float2>();
+        if (plan->fast) {
+            bpr_cols_forward<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(raw, sc, g, plan->root1, u0);
+            MS3_LAUNCH_CHECK();
+            bpr_rows_filter<kFastSA, kFastSB><<<g2, kFastSA * G, fsm2, stream>>>(sc, g, plan->root2, plan->twL,
+                                                                                 plan->kern);
+            MS3_LAUNCH_CHECK();
+            bpr_cols_inverse<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0);
+            MS3_LAUNCH_CHECK();
+        } else {
+            bp_cols_forward<<<g1, kThreads, sm1, stream>>>(raw, sc, g, plan->P1, plan->tw1, u0);
+            MS3_LAUNCH_CHECK();
+            bp_rows_filter<<<g2, kThreads, sm2, stream>>>(sc, g, plan->P2, plan->tw2, plan->twL, plan->kern);
+            MS3_LAUNCH_CHECK();
+            bp_cols_inverse<<<g1, kThreads, sm1, stream>>>(sc, out, g, plan->P1, plan->tw1, u0);
+            MS3_LAUNCH_CHECK();
+        }
     }
 }
 

@@ -284,8 +284,11 @@ __global__ void __launch_bounds__(256) apply_gemm(const float* __restrict__ X, c
                                                   int64_t M, int64_t N, double qunit, void* __restrict__ out) {
     __shared__ __align__(16) float Xs[kBK][kBM + 4];
     __shared__ __align__(16) float Ws[kBK][kBN + 4];
-    const int64_t t0 = (int64_t)blockIdx.x * kBM;
-    const int64_t n0 = (int64_t)blockIdx.y * kBN;
+    // column blocks of one time tile are adjacent in launch order, so the
+    // time tile of X is read from DRAM once and from L2 by the others
+    const int64_t ncb = (M + kBN - 1) / kBN;
+    const int64_t t0 = ((int64_t)blockIdx.x / ncb) * kBM;
+    const int64_t n0 = ((int64_t)blockIdx.x % ncb) * kBN;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     float acc[4][4];
 #pragma unroll
@@ -425,11 +428,9 @@ void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* 
     DevBuf wt(sizeof(float) * (size_t)(M * M), stream);
     w_to_float<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, wt.as<float>());
     MS3_LAUNCH_CHECK();
-    const int64_t gx = ceil_div(N, kBM);
-    const int64_t gy = ceil_div(M, kBN);
-    if (gy > 65535) throw_unsupported("too many channels for the apply kernel");
-    if (gx > 0x7fffffff) throw_unsupported("too many timepoints for the apply kernel");
-    apply_gemm<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, out);
+    const int64_t blocks = ceil_div(N, kBM) * ceil_div(M, kBN);
+    if (blocks > 0x7fffffff) throw_unsupported("too many tiles for the apply kernel");
+    apply_gemm<<<(unsigned)blocks, 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, out);
     MS3_LAUNCH_CHECK();
 }
 

@@ -55,6 +55,22 @@ def test_bandpass_parity(gpu_lib, ref32, M, N, T):
     assert rel(got, ref) <= 2e-6  # what accurate FP32 FFTs give
 
 
+def test_bandpass_generic_path_matches_register_path(gpu_lib, ref32, rec32):
+    # L = 240000 runs the register-pass kernels; MS3GPU_BP_GENERIC=1 forces the
+    # generic shared-memory Stockham kernels on the same window (fresh plan:
+    # a different freq_wid keys a new plan).
+    ref = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, 999.0, num_threads=16)
+    fast = api.bandpass_filter(rec32, FS, FMIN, FMAX, 999.0, num_threads=16)
+    os.environ["MS3GPU_BP_GENERIC"] = "1"
+    try:
+        gen = api.bandpass_filter(rec32, FS, FMIN, FMAX, 998.0, num_threads=16)
+    finally:
+        del os.environ["MS3GPU_BP_GENERIC"]
+    ref2 = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, 998.0, num_threads=16)
+    assert rel(fast, ref) <= 2e-6
+    assert rel(gen, ref2) <= 2e-6
+
+
 def test_bandpass_device_pointers_and_determinism(gpu_lib, rec32):
     import torch
 
