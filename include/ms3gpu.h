@@ -128,6 +128,28 @@ MS3GPU_API int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_
 MS3GPU_API int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt,
                              void* stream);
 
+/* Whiten pass 1 that allocates no memory.  No counterpart in the reference.
+ *
+ * Some callers cannot let the library call cudaMalloc: applications that
+ * hand the whole GPU to their own memory pool before processing starts (an
+ * extra allocation fails or fragments that pool), and streaming pipelines
+ * whose processing loop must not stall on a device allocation, which may
+ * synchronise the device.  This entry point computes the same XXt as
+ * ms3gpu_whiten_covariance but keeps its partial sums in a fixed 16 MiB
+ * array that is part of the library's device image (every GPU that loads the
+ * library holds it until the process exits); it allocates nothing.
+ *
+ * timeseries and XXt must be device memory of the current device (host
+ * buffers would need staging, which allocates); other pointers are rejected
+ * with MS3GPU_ERR_INVALID, and so is M above 1984 channels, the most whose
+ * 64 x 64 partial tiles fit the array.  The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one array, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialise
+ * them.  Each call overwrites every part of the array it reads. */
+MS3GPU_API int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t N, double* XXt,
+                                                void* stream);
+
 /* Stage: whitening_matrix_from_XXt (packages/ms3/pca.cpp:635-651) with
  * pca_from_XXt (:172-195): M components of 10 power iterations each from
  * the start vector sin(1..M), deflation (I-cc')XXt(I-cc'), W = C D C' with

@@ -66,6 +66,7 @@ SIGNATURES = {
     "ms3gpu_bandpass_whiten": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, ctypes.POINTER(BandpassOpts),
                                               ctypes.POINTER(WhitenOpts), _vp]),
     "ms3gpu_whiten_covariance": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
+    "ms3gpu_whiten_covariance_noalloc": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
     "ms3gpu_whitening_matrix": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, _vp, _vp]),
 }

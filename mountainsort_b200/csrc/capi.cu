@@ -287,6 +287,22 @@ int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, doub
     });
 }
 
+int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t N, double* XXt,
+                                     void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        cudaStream_t s = as_stream(stream);
+        require(timeseries, "timeseries", M * N > 0);
+        require(XXt, "XXt", M > 0);
+        // Staging host memory would allocate device buffers: only device memory is accepted.
+        if (M * N > 0 && !is_device_ptr(timeseries))
+            throw_invalid("ms3gpu_whiten_covariance_noalloc needs timeseries in device memory");
+        if (M > 0 && !is_device_ptr(XXt)) throw_invalid("ms3gpu_whiten_covariance_noalloc needs XXt in device memory");
+        covariance_device_noalloc(timeseries, M, N, XXt, s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* components, double* sigma,
                             void* stream) {
     return guarded([&] {

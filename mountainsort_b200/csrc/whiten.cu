@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 
 #include "common.cuh"
 #include "whiten.h"
@@ -365,6 +366,71 @@ void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaSt
     const int64_t total = (int64_t)npairs * kCT * kCT;
     cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(partials.as<double>(), (int)S, npairs, nb,
                                                                    M, N, XXt);
+    MS3_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------ covariance without allocation
+//
+// Scratch for the partial covariance tiles of ms3gpu_whiten_covariance_noalloc:
+// a fixed array in the library's device image, present on every GPU that
+// loads the library until the process exits.  Host code cannot use the
+// symbol's name as a device address; its address is looked up once per
+// device with cudaGetSymbolAddress and passed to the kernels.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_cov_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device (looked up on
+// the first call for that device).
+double* noalloc_scratch() {
+    int dev = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw_unsupported("device index above 63");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        MS3_CUDA(cudaGetSymbolAddress(&p, g_noalloc_cov_scratch));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+int64_t covariance_noalloc_max_channels() {
+    // the scratch must hold one time slice of 64 x 64 FP64 tiles of the upper triangle
+    const size_t tile = (size_t)kCT * kCT * sizeof(double);
+    int64_t nb = 1;
+    while ((size_t)(nb + 1) * (nb + 2) / 2 * tile <= kNoAllocScratchBytes) nb++;
+    return nb * kCT;
+}
+
+void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream) {
+    if (M <= 0) return;
+    if (M > covariance_noalloc_max_channels())
+        throw_invalid("ms3gpu_whiten_covariance_noalloc handles at most " +
+                      std::to_string(covariance_noalloc_max_channels()) + " channels (16 MiB scratch); got " +
+                      std::to_string(M));
+    double* scratch = noalloc_scratch();
+    const int nb = (int)ceil_div(M, kCT);
+    const int npairs = nb * (nb + 1) / 2;
+    if (N == 0) {
+        MS3_CUDA(cudaMemsetAsync(XXt, 0, sizeof(double) * (size_t)(M * M), stream));
+        return;
+    }
+    const int64_t s_max = (int64_t)(kNoAllocScratchBytes / ((size_t)npairs * kCT * kCT * sizeof(double)));
+    const int64_t target = std::max<int64_t>(1, (int64_t)4 * num_sms() / npairs);
+    int64_t S = std::min<int64_t>(std::min(target, s_max), ceil_div(N, kTT));
+    const int64_t tslice = ceil_div(ceil_div(N, S), kTT) * kTT;
+    S = ceil_div(N, tslice);
+    // Every partial tile the reduction reads is written by cov_partial in this
+    // call, so nothing left in the array by an earlier call is ever used.
+    cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, scratch);
+    MS3_LAUNCH_CHECK();
+    const int64_t total = (int64_t)npairs * kCT * kCT;
+    cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(scratch, (int)S, npairs, nb, M, N, XXt);
     MS3_LAUNCH_CHECK();
 }
 

@@ -10,6 +10,11 @@ namespace ms3gpu {
 // XXt (M x M doubles, column-major) = sum_t x_t x_t^T / (N-1 if N > 1).
 void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
 
+// The same covariance with its partial sums in a fixed 16 MiB device array
+// instead of allocated scratch (X and XXt must be device memory).
+void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
+int64_t covariance_noalloc_max_channels();
+
 // Power-iteration whitening matrix; comps / sigma may be null.
 void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
                              cudaStream_t stream);
