@@ -1,0 +1,309 @@
+// Whitening apply on the 5th-generation tensor cores (tcgen05, TMEM).
+//
+// y_t = W^T x_t for every timepoint (p_whiten.cpp:174-183: out[m1] +=
+// in[m2] * W[m1*M + m2]), then the reference's 1e-4 rounding and optional
+// int16 scaling.  As a GEMM: OUT[t][m1] = sum_m2 X[t][m2] * Wt[m1][m2] with
+// Wt[m1][m2] = W[m1*M + m2]; X (rows of M channels) and Wt are both K-major.
+//
+// Precision: three TF32 products per term, accumulated in FP32 in TMEM:
+//     x w ~= x_hi w_hi + x_hi w_lo + x_lo w_hi
+// x_hi is x truncated to TF32 (what the tensor core reads from the raw FP32
+// tile that TMA delivers), x_lo = rna_tf32(x - x_hi) is computed in shared
+// memory by a converter warpgroup; w_hi = rna_tf32(w), w_lo = rna_tf32(w - w_hi)
+// are prepared once per call.  The representation error is ~2^-22 of each
+// term, the same order as the reference's own float accumulation.
+//
+// One CTA computes a 128 (timepoints) x BN (channels) output tile:
+//   warp 0      TMA producer: X, Wt_hi, Wt_lo K-blocks of 32 into an
+//               S-stage ring (128-byte swizzle, the UMMA canonical layout)
+//   warp 1      TMEM allocation; one thread issues 3 MMAs per K=8 step and
+//               commits each stage back to the producer
+//   warps 4..7  convert X to X_lo per stage, then drain the accumulator
+//               (tcgen05.ld), round, store
+// Every mbarrier wait is bounded (tc::mbar_wait); a timeout raises *err.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+
+#include "common.cuh"
+#include "ms3gpu.h"
+#include "tc_sm100.cuh"
+#include "whiten.h"
+
+namespace ms3gpu {
+
+namespace {
+
+constexpr int kTM = 128;       // timepoints per tile (MMA M)
+constexpr int kKB = 32;        // K elements per stage (one 128-byte row)
+constexpr int kThreadsTC = 256;
+
+template <int BN>
+struct TcCfg {
+    static constexpr int kStages = (BN <= 128) ? 3 : 2;
+    static constexpr int kABytes = kTM * 128;  // 16 KB
+    static constexpr int kBBytes = BN * 128;
+    static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // X, X_lo, W_hi, W_lo
+    static constexpr int kTmemCols = (BN <= 32) ? 32 : (BN <= 64) ? 64 : (BN <= 128) ? 128 : 256;
+    static constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+};
+
+__device__ __forceinline__ float quantize_1e4_tc(float x) {
+    const double xd = (double)x;
+    double t = __dadd_rn(__dmul_rn(xd, 10000.0), 0.5);
+    double f = floor(t);
+    if (t - f < 1e-6 || f + 1.0 - t < 1e-6) {
+        t = __dadd_rn(__ddiv_rn(xd, 0.0001), 0.5);
+        f = floor(t);
+    }
+    return (float)__dmul_rn(f, 0.0001);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreadsTC, 1)
+    apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
+                    const __grid_constant__ CUtensorMap tmWlo, int64_t M, int64_t N, int ncb, double qunit,
+                    void* __restrict__ out, int* __restrict__ err) {
+    using C = TcCfg<BN>;
+    constexpr int S = C::kStages;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * C::kStageBytes);
+    uint64_t* full = bars;           // TMA bytes landed
+    uint64_t* conv = bars + S;       // X_lo written
+    uint64_t* empty = bars + 2 * S;  // MMAs done reading the stage
+    uint64_t* done = bars + 3 * S;   // all MMAs done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t tile = blockIdx.x / ncb;
+    const int cb = (int)(blockIdx.x % ncb);
+    const int64_t t0 = tile * kTM;
+    const int n0 = cb * BN;
+    const int nkb = (int)((M + kKB - 1) / kKB);
+
+    auto stageA = [&](int s) { return smem + (size_t)s * C::kStageBytes; };
+    auto stageAlo = [&](int s) { return smem + (size_t)s * C::kStageBytes + C::kABytes; };
+    auto stageBhi = [&](int s) { return smem + (size_t)s * C::kStageBytes + 2 * C::kABytes; };
+    auto stageBlo = [&](int s) { return smem + (size_t)s * C::kStageBytes + 2 * C::kABytes + C::kBBytes; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&conv[s], 128);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(done, 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 1) tc::tmem_alloc(tmem_slot, C::kTmemCols);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t taddr = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < nkb; kb++) {
+                const int s = kb % S;
+                if (kb >= S && !tc::mbar_wait(&empty[s], ((kb / S) - 1) & 1, err)) break;
+                tc::mbar_expect_tx(&full[s], C::kABytes + 2 * C::kBBytes);
+                tc::tma_load_2d(stageA(s), &tmX, &full[s], kb * kKB, (int)t0);
+                tc::tma_load_2d(stageBhi(s), &tmWhi, &full[s], kb * kKB, n0);
+                tc::tma_load_2d(stageBlo(s), &tmWlo, &full[s], kb * kKB, n0);
+                issued = kb + 1;
+            }
+            // no copy may still be landing in shared memory when the CTA exits
+            for (int kb = (issued > S ? issued - S : 0); kb < issued; kb++) tc::mbar_wait(&full[kb % S], (kb / S) & 1, err);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = tc::instr_desc(2u /*TF32*/, kTM, BN);
+            bool ok = true;
+            for (int kb = 0; kb < nkb && ok; kb++) {
+                const int s = kb % S;
+                ok = tc::mbar_wait(&full[s], (kb / S) & 1, err) && tc::mbar_wait(&conv[s], (kb / S) & 1, err);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint32_t a = tc::smem_u32(stageA(s)), al = tc::smem_u32(stageAlo(s));
+                const uint32_t bh = tc::smem_u32(stageBhi(s)), bl = tc::smem_u32(stageBlo(s));
+#pragma unroll
+                for (int ks = 0; ks < kKB / 8; ks++) {
+                    const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K inside the swizzle atom
+                    const uint64_t da = tc::smem_desc_k_sw128(a + off), dal = tc::smem_desc_k_sw128(al + off);
+                    const uint64_t dbh = tc::smem_desc_k_sw128(bh + off), dbl = tc::smem_desc_k_sw128(bl + off);
+                    tc::mma_tf32(taddr, da, dbh, idesc, (kb | ks) != 0);
+                    tc::mma_tf32(taddr, da, dbl, idesc, 1);
+                    tc::mma_tf32(taddr, dal, dbh, idesc, 1);
+                }
+                tc::mma_commit(&empty[s]);
+            }
+            tc::mma_commit(done);
+            // no MMA may still be writing TMEM when it is freed
+            tc::mbar_wait(done, 0, err);
+        }
+    } else if (warp >= 4) {
+        const int ct = threadIdx.x - 128;
+        bool ok = true;
+        for (int kb = 0; kb < nkb; kb++) {
+            const int s = kb % S;
+            if (!tc::mbar_wait(&full[s], (kb / S) & 1, err)) {
+                ok = false;
+                break;
+            }
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(stageA(s));
+            uint32_t* dst = reinterpret_cast<uint32_t*>(stageAlo(s));
+#pragma unroll 4
+            for (int i = ct; i < kTM * kKB; i += 128) {
+                const uint32_t xb = src[i];
+                const float x = __uint_as_float(xb);
+                const float hi = __uint_as_float(xb & 0xFFFFE000u);
+                dst[i] = tc::cvt_rna_tf32(x - hi);
+            }
+            tc::fence_proxy_async_smem();
+            tc::mbar_arrive(&conv[s]);
+        }
+        // epilogue: TMEM -> registers -> 1e-4 rounding -> global
+        if (ok) ok = tc::mbar_wait(done, 0, err);
+        if (__all_sync(0xffffffffu, ok)) {
+            tc::tc_fence_after();
+            const int q = warp & 3;
+            const int row = q * 32 + lane;
+            const int64_t t = t0 + row;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t r[32];
+                tc::tmem_ld_32x32b_x32(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, r);
+                if (t >= N) continue;
+                const int64_t nbase = (int64_t)n0 + c0;
+                if (qunit > 0) {
+                    int16_t* o16 = static_cast<int16_t*>(out) + t * M;
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        if (nbase + j >= M) break;
+                        const float y = quantize_1e4_tc(__uint_as_float(r[j]));
+                        const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)y, qunit), 0.5));
+                        o16[nbase + j] = x86_float_to_int16((float)iv);
+                    }
+                } else {
+                    float* of = static_cast<float*>(out) + t * M + nbase;
+                    if (nbase + 32 <= M && ((reinterpret_cast<uintptr_t>(of) & 15) == 0)) {
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4) {
+                            float4 v;
+                            v.x = quantize_1e4_tc(__uint_as_float(r[j]));
+                            v.y = quantize_1e4_tc(__uint_as_float(r[j + 1]));
+                            v.z = quantize_1e4_tc(__uint_as_float(r[j + 2]));
+                            v.w = quantize_1e4_tc(__uint_as_float(r[j + 3]));
+                            *reinterpret_cast<float4*>(of + j) = v;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            if (nbase + j >= M) break;
+                            of[j] = quantize_1e4_tc(__uint_as_float(r[j]));
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(taddr, C::kTmemCols);
+    }
+}
+
+// w_hi = rna_tf32(w), w_lo = rna_tf32(w - w_hi) of Wt[m1][m2] = W[m1*M + m2].
+__global__ void w_split_tf32(const double* __restrict__ W, int64_t MM, float* __restrict__ hi, float* __restrict__ lo) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MM) return;
+    const double w = W[i];
+    const float h = __uint_as_float(tc::cvt_rna_tf32((float)w));
+    hi[i] = h;
+    lo[i] = __uint_as_float(tc::cvt_rna_tf32((float)(w - (double)h)));
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static cudaError_t status = cudaSuccess;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        status = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (status == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) throw_unsupported("cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+// Row-major [rows][cols] float32 matrix, tiles of box_rows x 32 columns, 128-byte swizzle.
+CUtensorMap make_map(const void* base, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kKB, box_rows};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(base), dims, strides, box,
+                                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw_unsupported("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+template <int BN>
+void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, const float* wlo, double qunit,
+                     void* out, int* err, cudaStream_t stream) {
+    using C = TcCfg<BN>;
+    MS3_CUDA(cudaFuncSetAttribute(apply_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)C::kSmemBytes));
+    const CUtensorMap mx = make_map(X, (uint64_t)M, (uint64_t)N, kTM);
+    const CUtensorMap mh = make_map(whi, (uint64_t)M, (uint64_t)M, BN);
+    const CUtensorMap ml = make_map(wlo, (uint64_t)M, (uint64_t)M, BN);
+    const int ncb = (int)ceil_div(M, BN);
+    const int64_t blocks = ceil_div(N, kTM) * ncb;
+    if (blocks > 0x7fffffff) throw_unsupported("too many tiles for the tensor-core apply");
+    apply_tc_kernel<BN><<<(unsigned)blocks, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, qunit, out,
+                                                                                err);
+    MS3_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out) {
+    const char* off = std::getenv("MS3GPU_APPLY_FFMA");
+    if (off && off[0] == '1') return false;
+    if (M < 4 || M % 4 != 0 || M > 65536 || N < 1) return false;  // TMA: 16-byte row strides
+    if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return false;
+    (void)out;
+    return true;
+}
+
+void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
+                        void* out, cudaStream_t stream) {
+    DevBuf wbuf(sizeof(float) * (size_t)(2 * M * M) + 256, stream);
+    float* whi = wbuf.as<float>();
+    float* wlo = whi + M * M;
+    int* err = reinterpret_cast<int*>(wlo + M * M);
+    MS3_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    w_split_tf32<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, whi, wlo);
+    MS3_LAUNCH_CHECK();
+    if (M <= 128)
+        launch_apply_tc<128>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+    else
+        launch_apply_tc<192>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+    int herr = 0;
+    MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    MS3_CUDA(cudaStreamSynchronize(stream));
+    if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+}
+
+}  // namespace ms3gpu

@@ -491,6 +491,10 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
                             void* out, cudaStream_t stream) {
     if (M <= 0 || N <= 0) return;
+    if (apply_tc_supported(X, M, N, out)) {
+        apply_whitening_tc(X, M, N, W, quantization_unit, out, stream);
+        return;
+    }
     DevBuf wt(sizeof(float) * (size_t)(M * M), stream);
     w_to_float<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, wt.as<float>());
     MS3_LAUNCH_CHECK();

@@ -24,4 +24,10 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W,
                             double quantization_unit, void* out, cudaStream_t stream);
 
+// Tensor-core (tcgen05, 3-term TF32) apply; apply_tc_supported tells whether
+// the shapes and alignment allow it.
+bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out);
+void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
+                        void* out, cudaStream_t stream);
+
 }  // namespace ms3gpu

@@ -177,6 +177,26 @@ def test_whitening_matrix_global_rows_match_shared(gpu_lib, M):
         np.testing.assert_allclose(W, W.T, rtol=0, atol=1e-12 * np.abs(W).max())
 
 
+def test_apply_tensor_core_vs_ffma_at_384(gpu_lib, ref32):
+    # 384 channels (the benchmark's shape): the tcgen05 3-term-TF32 apply and
+    # the FP32 FMA apply both within the plain-form gate of ref32's apply.
+    M, N = 384, 20000
+    X = synth.generate_numpy(M, N, K=40, seed=384, sites=(6, 12))
+    C = o64.xxt(X)
+    W, _, _ = o64.whitening_matrix(C)
+    ref = ref32.whiten_apply(X, W)
+    tcv = api.apply_whitening_matrix(X, W)
+    os.environ["MS3GPU_APPLY_FFMA"] = "1"
+    try:
+        ffma = api.apply_whitening_matrix(X, W)
+    finally:
+        del os.environ["MS3GPU_APPLY_FFMA"]
+    e_tc, e_ffma = rel(tcv, ref), rel(ffma, ref)
+    print(f"apply rel L2 vs ref32: tensor core {e_tc:.3e}, FP32 FMA {e_ffma:.3e}")
+    assert e_ffma <= 1e-5
+    assert e_tc <= 1e-5
+
+
 def test_whiten_int16(gpu_lib, ref32, rec32):
     F = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
     ref, _, _ = ref32.whiten(F, quantization_unit=0.01)
