@@ -1,10 +1,11 @@
 // sm_100a primitives: mbarriers, TMA tile loads, TMEM allocation, tcgen05
 // MMA / commit / load.  Inline PTX, one instruction per wrapper.
 //
-// Every wait on an mbarrier is bounded: after kMaxTries failed try_wait
-// probes the waiting thread raises a flag in global memory and gives up, so a
-// broken pipeline ends the kernel with an error status instead of hanging the
-// GPU.  Callers check the flag after the launch.
+// Every wait on an mbarrier is bounded: after kTimeoutNs of failed try_wait
+// probes (measured on %globaltimer) the waiting thread raises a flag in
+// global memory and gives up, so a broken pipeline ends the kernel with an
+// error status instead of hanging the GPU.  Callers check the flag after the
+// launch.
 #pragma once
 
 #include <cuda.h>
@@ -15,7 +16,13 @@
 namespace ms3gpu {
 namespace tc {
 
-constexpr long long kMaxTries = 1LL << 22;  // each try_wait may suspend ~us: seconds in total
+constexpr unsigned long long kTimeoutNs = 2000000000ULL;  // 2 s
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -53,12 +60,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Bounded wait for the phase with the given parity.  Returns false (and sets
 // *err) on timeout or when another thread has already failed.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (long long i = 0; i < kMaxTries; i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 1023) == 1023 && *reinterpret_cast<volatile int*>(err)) return false;
+        if (*reinterpret_cast<volatile int*>(err)) return false;
+        if (globaltimer_ns() - t0 > kTimeoutNs) {
+            atomicExch(err, 1);
+            return false;
+        }
     }
-    atomicExch(err, 1);
-    return false;
 }
 
 // 2-D TMA tile load global -> shared, completion counted on `bar` (bytes).
