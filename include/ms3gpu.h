@@ -67,9 +67,15 @@ typedef struct ms3gpu_bandpass_opts {
     int32_t num_threads;      /* T of the chunk-size formula; must be >= 1 */
 } ms3gpu_bandpass_opts;
 
-/* Whiten_opts (packages/ms3/p_whiten.h:21-26). */
+/* Arithmetic of the whitening passes. */
+#define MS3GPU_PRECISION_PLAIN 0 /* FP32 FMA apply: parity with the reference (<= 1e-5 rel. L2) */
+#define MS3GPU_PRECISION_MIXED 1 /* tensor-core 3-term TF32 apply (tcgen05), FP32 accumulation:
+                                    <= 1e-4 rel. L2 against the FP64 algorithm */
+
+/* Whiten_opts (packages/ms3/p_whiten.h:21-26) plus the arithmetic mode. */
 typedef struct ms3gpu_whiten_opts {
     double quantization_unit; /* > 0: int16 output of round(y / quantization_unit) */
+    int32_t precision;        /* MS3GPU_PRECISION_PLAIN (default) or MS3GPU_PRECISION_MIXED */
 } ms3gpu_whiten_opts;
 
 /* Text of the last error on the calling thread ("" if none). */
@@ -160,9 +166,11 @@ MS3GPU_API int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, 
 
 /* Stage: whiten pass 2 (p_whiten.cpp:153-206): out(m1, t) = sum_m2
  * x(m2, t) W[m1*M + m2], rounded to multiples of 1e-4 (:31-41), then
- * int16 (int)(y/q + 0.5) when quantization_unit > 0 (:445-451). */
+ * int16 (int)(y/q + 0.5) when quantization_unit > 0 (:445-451).
+ * precision: MS3GPU_PRECISION_PLAIN or MS3GPU_PRECISION_MIXED. */
 MS3GPU_API int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N, const double* W,
-                                  double quantization_unit, void* timeseries_out, void* stream);
+                                  double quantization_unit, int32_t precision, void* timeseries_out,
+                                  void* stream);
 
 #ifdef __cplusplus
 }

@@ -34,9 +34,13 @@ class BandpassOpts(ctypes.Structure):
     ]
 
 
+PRECISION_PLAIN = 0
+PRECISION_MIXED = 1
+
+
 class WhitenOpts(ctypes.Structure):
-    """ms3gpu_whiten_opts (Whiten_opts, p_whiten.h:21-26)."""
-    _fields_ = [("quantization_unit", ctypes.c_double)]
+    """ms3gpu_whiten_opts (Whiten_opts, p_whiten.h:21-26, plus precision)."""
+    _fields_ = [("quantization_unit", ctypes.c_double), ("precision", ctypes.c_int32)]
 
 
 class Ms3GpuError(RuntimeError):
@@ -68,7 +72,7 @@ SIGNATURES = {
     "ms3gpu_whiten_covariance": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
     "ms3gpu_whiten_covariance_noalloc": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
     "ms3gpu_whitening_matrix": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
-    "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, _vp, _vp]),
+    "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
 }
 
 _lib = None

@@ -112,27 +112,33 @@ def bandpass_filter(X, samplerate, freq_min, freq_max, freq_wid=1000.0, quantiza
     return out
 
 
-def whiten(X, quantization_unit=0.0, out=None, stream=None):
-    """ms3.whiten (packages/ms3/p_whiten.cpp:45-206) on an (N, M) array."""
+_PRECISION = {"plain": _lib.PRECISION_PLAIN, "mixed": _lib.PRECISION_MIXED}
+
+
+def whiten(X, quantization_unit=0.0, out=None, stream=None, precision="plain"):
+    """ms3.whiten (packages/ms3/p_whiten.cpp:45-206) on an (N, M) array.
+    precision "plain" (FP32, parity with the reference) or "mixed"
+    (tensor-core 3-term TF32 apply)."""
     L = _lib.load()
     X = _as_f32_rows(X)
     N, M = X.shape
     if out is None:
         out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
-    o = WhitenOpts(float(quantization_unit))
+    o = WhitenOpts(float(quantization_unit), _PRECISION[precision])
     check(L.ms3gpu_whiten(_ptr(X), M, N, _ptr(out), ctypes.byref(o), _stream_ptr(X, stream)))
     return out
 
 
 def bandpass_whiten(X, samplerate, freq_min, freq_max, freq_wid=1000.0, num_threads=None,
-                    quantization_unit=0.0, filt_out=None, out=None, want_filt=False, stream=None):
+                    quantization_unit=0.0, filt_out=None, out=None, want_filt=False, stream=None,
+                    precision="plain"):
     """ms3.bandpass_filter followed by ms3.whiten, as mountainsort3.mlp runs
     them.  Returns pre, or (filt, pre) when want_filt or filt_out is given."""
     L = _lib.load()
     X = _as_f32_rows(X)
     N, M = X.shape
     bp = bandpass_opts(samplerate, freq_min, freq_max, freq_wid, 0.0, 1, num_threads)
-    wh = WhitenOpts(float(quantization_unit))
+    wh = WhitenOpts(float(quantization_unit), _PRECISION[precision])
     if want_filt and filt_out is None:
         filt_out = _empty_like(X, (N, M), np.float32)
     if out is None:
@@ -167,7 +173,7 @@ def whitening_matrix(XXt, stream=None, return_components=False):
     return _mat_out(W)
 
 
-def apply_whitening_matrix(X, W, quantization_unit=0.0, out=None, stream=None):
+def apply_whitening_matrix(X, W, quantization_unit=0.0, out=None, stream=None, precision="plain"):
     """Whiten pass 2 (p_whiten.cpp:153-206) with a given W."""
     L = _lib.load()
     X = _as_f32_rows(X)
@@ -175,8 +181,8 @@ def apply_whitening_matrix(X, W, quantization_unit=0.0, out=None, stream=None):
     Wc = _mat_in(W, X)
     if out is None:
         out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
-    check(L.ms3gpu_apply_whitening_matrix(_ptr(X), M, N, _ptr(Wc), float(quantization_unit), _ptr(out),
-                                          _stream_ptr(X, stream)))
+    check(L.ms3gpu_apply_whitening_matrix(_ptr(X), M, N, _ptr(Wc), float(quantization_unit),
+                                          _PRECISION[precision], _ptr(out), _stream_ptr(X, stream)))
     return out
 
 

@@ -42,13 +42,16 @@ constexpr int kTM = 128;       // timepoints per tile (MMA M)
 constexpr int kKB = 32;        // K elements per stage (one 128-byte row)
 constexpr int kThreadsTC = 256;
 
-template <int BN>
+template <int BN, bool DRAIN>
 struct TcCfg {
     static constexpr int kStages = (BN <= 128) ? 3 : 2;
     static constexpr int kABytes = kTM * 128;  // 16 KB
     static constexpr int kBBytes = BN * 128;
     static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // X, X_lo, W_hi, W_lo
-    static constexpr int kTmemCols = (BN <= 32) ? 32 : (BN <= 64) ? 64 : (BN <= 128) ? 128 : 256;
+    // DRAIN: two hi*hi accumulators (alternate K-blocks) + one for the small terms
+    static constexpr int kUsedCols = DRAIN ? 3 * BN : BN;
+    static constexpr int kTmemCols = (kUsedCols <= 32) ? 32 : (kUsedCols <= 64) ? 64 : (kUsedCols <= 128) ? 128
+                                     : (kUsedCols <= 256) ? 256 : 512;
     static constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 };
 
@@ -63,21 +66,65 @@ __device__ __forceinline__ float quantize_1e4_tc(float x) {
     return (float)__dmul_rn(f, 0.0001);
 }
 
-template <int BN>
+// Rounds and stores 32 consecutive output channels of one timepoint.
+__device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int64_t nbase, int64_t M, double qunit,
+                                            void* __restrict__ out) {
+    if (qunit > 0) {
+        int16_t* o16 = static_cast<int16_t*>(out) + t * M;
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            if (nbase + j >= M) break;
+            const float q = quantize_1e4_tc(y[j]);
+            const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)q, qunit), 0.5));
+            o16[nbase + j] = x86_float_to_int16((float)iv);
+        }
+        return;
+    }
+    float* of = static_cast<float*>(out) + t * M + nbase;
+    if (nbase + 32 <= M && ((reinterpret_cast<uintptr_t>(of) & 15) == 0)) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+            float4 v;
+            v.x = quantize_1e4_tc(y[j]);
+            v.y = quantize_1e4_tc(y[j + 1]);
+            v.z = quantize_1e4_tc(y[j + 2]);
+            v.w = quantize_1e4_tc(y[j + 3]);
+            *reinterpret_cast<float4*>(of + j) = v;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            if (nbase + j >= M) break;
+            of[j] = quantize_1e4_tc(y[j]);
+        }
+    }
+}
+
+// DRAIN = false (mixed form): all three products accumulate over the whole K
+// range in one FP32 TMEM accumulator.
+// DRAIN = true (plain form): the tensor core's FP32 accumulation rounds
+// toward zero, so long accumulations of the large hi*hi terms drift.  Each
+// K-block's hi*hi products go to a fresh accumulator (two, alternating) that
+// the epilogue warps drain into round-to-nearest FP32 sums while the next
+// K-block runs; the small hi*lo + lo*hi terms keep one long-lived
+// accumulator (their rounding is ~2^-11 smaller).
+template <int BN, bool DRAIN>
 __global__ void __launch_bounds__(kThreadsTC, 1)
     apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
                     const __grid_constant__ CUtensorMap tmWlo, int64_t M, int64_t N, int ncb, double qunit,
                     void* __restrict__ out, int* __restrict__ err) {
-    using C = TcCfg<BN>;
+    using C = TcCfg<BN, DRAIN>;
     constexpr int S = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * C::kStageBytes);
-    uint64_t* full = bars;           // TMA bytes landed
-    uint64_t* conv = bars + S;       // X_lo written
-    uint64_t* empty = bars + 2 * S;  // MMAs done reading the stage
-    uint64_t* done = bars + 3 * S;   // all MMAs done
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 1);
+    uint64_t* full = bars;               // TMA bytes landed
+    uint64_t* conv = bars + S;           // X_lo written
+    uint64_t* empty = bars + 2 * S;      // MMAs done reading the stage
+    uint64_t* done = bars + 3 * S;       // all MMAs done
+    uint64_t* acc_full = bars + 3 * S + 1;  // [2] hi*hi K-block accumulator ready (DRAIN)
+    uint64_t* acc_free = bars + 3 * S + 3;  // [2] accumulator drained (DRAIN)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 5);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t tile = blockIdx.x / ncb;
@@ -94,10 +141,14 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) {
             tc::mbar_init(&full[s], 1);
-            tc::mbar_init(&conv[s], 128);
+            tc::mbar_init(&conv[s], 64);
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(done, 1);
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&acc_full[b], 1);
+            tc::mbar_init(&acc_free[b], 128);
+        }
         tc::fence_mbar_init();
     }
     if (warp == 1) tc::tmem_alloc(tmem_slot, C::kTmemCols);
@@ -105,6 +156,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t taddr = *tmem_slot;
+    const uint32_t acc_big[2] = {taddr, taddr + (uint32_t)BN};
+    const uint32_t acc_small = DRAIN ? taddr + 2u * BN : taddr;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -119,7 +172,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 issued = kb + 1;
             }
             // no copy may still be landing in shared memory when the CTA exits
-            for (int kb = (issued > S ? issued - S : 0); kb < issued; kb++) tc::mbar_wait(&full[kb % S], (kb / S) & 1, err);
+            for (int kb = (issued > S ? issued - S : 0); kb < issued; kb++)
+                tc::mbar_wait(&full[kb % S], (kb / S) & 1, err);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -127,7 +181,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             bool ok = true;
             for (int kb = 0; kb < nkb && ok; kb++) {
                 const int s = kb % S;
+                const int b = kb & 1;
                 ok = tc::mbar_wait(&full[s], (kb / S) & 1, err) && tc::mbar_wait(&conv[s], (kb / S) & 1, err);
+                if (ok && DRAIN && kb >= 2) ok = tc::mbar_wait(&acc_free[b], ((kb >> 1) - 1) & 1, err);
                 if (!ok) break;
                 tc::tc_fence_after();
                 const uint32_t a = tc::smem_u32(stageA(s)), al = tc::smem_u32(stageAlo(s));
@@ -137,29 +193,32 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                     const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K inside the swizzle atom
                     const uint64_t da = tc::smem_desc_k_sw128(a + off), dal = tc::smem_desc_k_sw128(al + off);
                     const uint64_t dbh = tc::smem_desc_k_sw128(bh + off), dbl = tc::smem_desc_k_sw128(bl + off);
-                    tc::mma_tf32(taddr, da, dbh, idesc, (kb | ks) != 0);
-                    tc::mma_tf32(taddr, da, dbl, idesc, 1);
-                    tc::mma_tf32(taddr, dal, dbh, idesc, 1);
+                    if (DRAIN) {
+                        tc::mma_tf32(acc_big[b], da, dbh, idesc, ks != 0);
+                        tc::mma_tf32(acc_small, da, dbl, idesc, (kb | ks) != 0);
+                    } else {
+                        tc::mma_tf32(acc_small, da, dbh, idesc, (kb | ks) != 0);
+                        tc::mma_tf32(acc_small, da, dbl, idesc, 1);
+                    }
+                    tc::mma_tf32(acc_small, dal, dbh, idesc, 1);
                 }
                 tc::mma_commit(&empty[s]);
+                if (DRAIN) tc::mma_commit(&acc_full[b]);
             }
             tc::mma_commit(done);
             // no MMA may still be writing TMEM when it is freed
             tc::mbar_wait(done, 0, err);
         }
-    } else if (warp >= 4) {
-        const int ct = threadIdx.x - 128;
-        bool ok = true;
+    } else if (warp < 4) {
+        // warps 2-3: X_lo = rna_tf32(x - trunc_tf32(x)), same swizzled layout as X
+        const int ct = threadIdx.x - 64;
         for (int kb = 0; kb < nkb; kb++) {
             const int s = kb % S;
-            if (!tc::mbar_wait(&full[s], (kb / S) & 1, err)) {
-                ok = false;
-                break;
-            }
+            if (!tc::mbar_wait(&full[s], (kb / S) & 1, err)) break;
             const uint32_t* src = reinterpret_cast<const uint32_t*>(stageA(s));
             uint32_t* dst = reinterpret_cast<uint32_t*>(stageAlo(s));
-#pragma unroll 4
-            for (int i = ct; i < kTM * kKB; i += 128) {
+#pragma unroll 8
+            for (int i = ct; i < kTM * kKB; i += 64) {
                 const uint32_t xb = src[i];
                 const float x = __uint_as_float(xb);
                 const float hi = __uint_as_float(xb & 0xFFFFE000u);
@@ -168,48 +227,46 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             tc::fence_proxy_async_smem();
             tc::mbar_arrive(&conv[s]);
         }
-        // epilogue: TMEM -> registers -> 1e-4 rounding -> global
+    } else {
+        // warps 4-7: accumulator drain and epilogue; warp q reads TMEM lanes 32q..32q+31
+        const int q = warp & 3;
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        const int64_t t = t0 + q * 32 + lane;
+        bool ok = true;
+        float sums[BN];
+#pragma unroll
+        for (int j = 0; j < BN; j++) sums[j] = 0.f;
+        if (DRAIN) {
+            for (int kb = 0; kb < nkb && ok; kb++) {
+                const int b = kb & 1;
+                ok = tc::mbar_wait(&acc_full[b], (kb >> 1) & 1, err);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    ok = false;
+                    break;
+                }
+                tc::tc_fence_after();
+#pragma unroll
+                for (int c0 = 0; c0 < BN; c0 += 32) {
+                    uint32_t r[32];
+                    tc::tmem_ld_32x32b_x32(acc_big[b] + lane_base + (uint32_t)c0, r);
+#pragma unroll
+                    for (int j = 0; j < 32; j++) sums[c0 + j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
+                }
+                tc::tc_fence_before();
+                tc::mbar_arrive(&acc_free[b]);
+            }
+        }
         if (ok) ok = tc::mbar_wait(done, 0, err);
         if (__all_sync(0xffffffffu, ok)) {
             tc::tc_fence_after();
-            const int q = warp & 3;
-            const int row = q * 32 + lane;
-            const int64_t t = t0 + row;
-#pragma unroll 1
+#pragma unroll
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 uint32_t r[32];
-                tc::tmem_ld_32x32b_x32(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, r);
-                if (t >= N) continue;
-                const int64_t nbase = (int64_t)n0 + c0;
-                if (qunit > 0) {
-                    int16_t* o16 = static_cast<int16_t*>(out) + t * M;
+                tc::tmem_ld_32x32b_x32(acc_small + lane_base + (uint32_t)c0, r);
+                float y[32];
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        if (nbase + j >= M) break;
-                        const float y = quantize_1e4_tc(__uint_as_float(r[j]));
-                        const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)y, qunit), 0.5));
-                        o16[nbase + j] = x86_float_to_int16((float)iv);
-                    }
-                } else {
-                    float* of = static_cast<float*>(out) + t * M + nbase;
-                    if (nbase + 32 <= M && ((reinterpret_cast<uintptr_t>(of) & 15) == 0)) {
-#pragma unroll
-                        for (int j = 0; j < 32; j += 4) {
-                            float4 v;
-                            v.x = quantize_1e4_tc(__uint_as_float(r[j]));
-                            v.y = quantize_1e4_tc(__uint_as_float(r[j + 1]));
-                            v.z = quantize_1e4_tc(__uint_as_float(r[j + 2]));
-                            v.w = quantize_1e4_tc(__uint_as_float(r[j + 3]));
-                            *reinterpret_cast<float4*>(of + j) = v;
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 32; j++) {
-                            if (nbase + j >= M) break;
-                            of[j] = quantize_1e4_tc(__uint_as_float(r[j]));
-                        }
-                    }
-                }
+                for (int j = 0; j < 32; j++) y[j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
+                if (t < N) store_row32(y, t, (int64_t)n0 + c0, M, qunit, out);
             }
         }
     }
@@ -259,11 +316,11 @@ CUtensorMap make_map(const void* base, uint64_t cols, uint64_t rows, uint32_t bo
     return m;
 }
 
-template <int BN>
+template <int BN, bool DRAIN>
 void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, const float* wlo, double qunit,
                      void* out, int* err, cudaStream_t stream) {
-    using C = TcCfg<BN>;
-    MS3_CUDA(cudaFuncSetAttribute(apply_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    using C = TcCfg<BN, DRAIN>;
+    MS3_CUDA(cudaFuncSetAttribute(apply_tc_kernel<BN, DRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)C::kSmemBytes));
     const CUtensorMap mx = make_map(X, (uint64_t)M, (uint64_t)N, kTM);
     const CUtensorMap mh = make_map(whi, (uint64_t)M, (uint64_t)M, BN);
@@ -271,16 +328,14 @@ void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, con
     const int ncb = (int)ceil_div(M, BN);
     const int64_t blocks = ceil_div(N, kTM) * ncb;
     if (blocks > 0x7fffffff) throw_unsupported("too many tiles for the tensor-core apply");
-    apply_tc_kernel<BN><<<(unsigned)blocks, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, qunit, out,
-                                                                                err);
+    apply_tc_kernel<BN, DRAIN><<<(unsigned)blocks, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, qunit,
+                                                                                       out, err);
     MS3_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out) {
-    const char* off = std::getenv("MS3GPU_APPLY_FFMA");
-    if (off && off[0] == '1') return false;
     if (M < 4 || M % 4 != 0 || M > 65536 || N < 1) return false;  // TMA: 16-byte row strides
     if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return false;
     (void)out;
@@ -288,7 +343,7 @@ bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out) {
 }
 
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        void* out, cudaStream_t stream) {
+                        bool drain, void* out, cudaStream_t stream) {
     DevBuf wbuf(sizeof(float) * (size_t)(2 * M * M) + 256, stream);
     float* whi = wbuf.as<float>();
     float* wlo = whi + M * M;
@@ -296,10 +351,12 @@ void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, d
     MS3_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
     w_split_tf32<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, whi, wlo);
     MS3_LAUNCH_CHECK();
-    if (M <= 128)
-        launch_apply_tc<128>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+    if (drain)
+        launch_apply_tc<128, true>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+    else if (M <= 128)
+        launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
     else
-        launch_apply_tc<192>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+        launch_apply_tc<192, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
     int herr = 0;
     MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
     MS3_CUDA(cudaStreamSynchronize(stream));

@@ -189,6 +189,12 @@ BandpassParams to_params(const ms3gpu_bandpass_opts* o) {
 
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
+bool check_precision(int32_t p) {
+    if (p != MS3GPU_PRECISION_PLAIN && p != MS3GPU_PRECISION_MIXED)
+        throw_invalid("precision must be MS3GPU_PRECISION_PLAIN (0) or MS3GPU_PRECISION_MIXED (1)");
+    return p == MS3GPU_PRECISION_MIXED;
+}
+
 }  // namespace
 }  // namespace ms3gpu
 
@@ -328,7 +334,8 @@ int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* com
 }
 
 int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N, const double* W,
-                                  double quantization_unit, void* timeseries_out, void* stream) {
+                                  double quantization_unit, int32_t precision, void* timeseries_out,
+                                  void* stream) {
     return guarded([&] {
         check_shape(M, N);
         cudaStream_t s = as_stream(stream);
@@ -343,7 +350,7 @@ int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N,
         OutView out;
         out.setup(timeseries_out, out_bytes, s);
         apply_whitening_device(static_cast<const float*>(in.ptr), M, N, static_cast<const double*>(w.ptr),
-                               quantization_unit, out.ptr, s);
+                               quantization_unit, check_precision(precision), out.ptr, s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
     });
@@ -369,7 +376,8 @@ int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeserie
         double* W = XXt + M * M;
         covariance_device(static_cast<const float*>(in.ptr), M, N, XXt, s);
         whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
-        apply_whitening_device(static_cast<const float*>(in.ptr), M, N, W, q, out.ptr, s);
+        apply_whitening_device(static_cast<const float*>(in.ptr), M, N, W, q, check_precision(opts->precision),
+                               out.ptr, s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
     });
@@ -410,7 +418,7 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         double* W = XXt + M * M;
         covariance_device(filt_d, M, N, XXt, s);
         whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
-        apply_whitening_device(filt_d, M, N, W, q, pre.ptr, s);
+        apply_whitening_device(filt_d, M, N, W, q, check_precision(wh->precision), pre.ptr, s);
         if (filt_out) filt.finish(s);
         pre.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));

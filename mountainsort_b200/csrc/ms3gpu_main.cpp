@@ -226,6 +226,8 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
     const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
     ms3gpu_whiten_opts o;
     o.quantization_unit = clp.num("quantization_unit", 0);  // mountainsort3_main.cpp:576
+    // --_precision=mixed selects the tensor-core apply (not a reference parameter)
+    o.precision = clp.str("_precision") == "mixed" ? MS3GPU_PRECISION_MIXED : MS3GPU_PRECISION_PLAIN;
     std::string err;
     ms3io::MdaHeader h;
     if (!ms3io::read_header(in, h, err)) return fail(err);

@@ -489,10 +489,13 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 }
 
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                            void* out, cudaStream_t stream) {
+                            bool mixed, void* out, cudaStream_t stream) {
     if (M <= 0 || N <= 0) return;
-    if (apply_tc_supported(X, M, N, out)) {
-        apply_whitening_tc(X, M, N, W, quantization_unit, out, stream);
+    // MS3GPU_APPLY_FFMA=1 selects the FP32 FMA kernel for the plain form
+    const char* ffma = std::getenv("MS3GPU_APPLY_FFMA");
+    const bool force_ffma = ffma && ffma[0] == '1';
+    if (apply_tc_supported(X, M, N, out) && (mixed || !force_ffma)) {
+        apply_whitening_tc(X, M, N, W, quantization_unit, /*drain=*/!mixed, out, stream);
         return;
     }
     DevBuf wt(sizeof(float) * (size_t)(M * M), stream);

@@ -20,14 +20,17 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
                              cudaStream_t stream);
 
 // out = quantize(W^T x) per timepoint; out float32, or int16 when
-// quantization_unit > 0.
+// quantization_unit > 0.  mixed: tensor-core 3-term TF32 (when the shapes
+// allow), else FP32 FMA.
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W,
-                            double quantization_unit, void* out, cudaStream_t stream);
+                            double quantization_unit, bool mixed, void* out, cudaStream_t stream);
 
 // Tensor-core (tcgen05, 3-term TF32) apply; apply_tc_supported tells whether
 // the shapes and alignment allow it.
 bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out);
+// drain: per-K-block draining of the large products into round-to-nearest
+// FP32 sums (plain form); otherwise one FP32 TMEM accumulator (mixed form).
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        void* out, cudaStream_t stream);
+                        bool drain, void* out, cudaStream_t stream);
 
 }  // namespace ms3gpu

@@ -177,24 +177,39 @@ def test_whitening_matrix_global_rows_match_shared(gpu_lib, M):
         np.testing.assert_allclose(W, W.T, rtol=0, atol=1e-12 * np.abs(W).max())
 
 
-def test_apply_tensor_core_vs_ffma_at_384(gpu_lib, ref32):
-    # 384 channels (the benchmark's shape): the tcgen05 3-term-TF32 apply and
-    # the FP32 FMA apply both within the plain-form gate of ref32's apply.
+def test_apply_plain_and_mixed_at_384(gpu_lib, ref32):
+    # 384 channels (the benchmark's shape).  Plain form (FP32 FMA): within
+    # 1e-5 of ref32's apply.  Mixed form (tcgen05, 3-term TF32, FP32
+    # accumulation in TMEM): within 1e-4 of the FP64 apply.
     M, N = 384, 20000
     X = synth.generate_numpy(M, N, K=40, seed=384, sites=(6, 12))
     C = o64.xxt(X)
     W, _, _ = o64.whitening_matrix(C)
     ref = ref32.whiten_apply(X, W)
-    tcv = api.apply_whitening_matrix(X, W)
+    exact = o64.quantize(X.astype(np.float64) @ W)
+    plain = api.apply_whitening_matrix(X, W)  # tcgen05 with drained accumulators
+    mixed = api.apply_whitening_matrix(X, W, precision="mixed")
     os.environ["MS3GPU_APPLY_FFMA"] = "1"
     try:
         ffma = api.apply_whitening_matrix(X, W)
     finally:
         del os.environ["MS3GPU_APPLY_FFMA"]
-    e_tc, e_ffma = rel(tcv, ref), rel(ffma, ref)
-    print(f"apply rel L2 vs ref32: tensor core {e_tc:.3e}, FP32 FMA {e_ffma:.3e}")
+    e_plain, e_ffma = rel(plain, ref), rel(ffma, ref)
+    e_mixed, e_mixed64 = rel(mixed, ref), rel(mixed, exact)
+    print(f"apply rel L2 vs ref32: plain tensor-core {e_plain:.3e}, plain FMA {e_ffma:.3e}, "
+          f"mixed {e_mixed:.3e} (mixed vs FP64 {e_mixed64:.3e})")
+    assert e_plain <= 1e-5
     assert e_ffma <= 1e-5
-    assert e_tc <= 1e-5
+    assert e_mixed64 <= 1e-4
+
+
+def test_mixed_pipeline_vs_fp64_oracle(gpu_lib, rec32):
+    # the mixed-precision form on config-1 geometry, gated against the FP64 oracle
+    pre = api.bandpass_whiten(rec32, FS, FMIN, FMAX, FWID, num_threads=16, precision="mixed")
+    y, q64, _, _ = o64.whiten(o64.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16))
+    err = rel(pre, q64)
+    print(f"mixed pipeline rel L2 vs FP64 oracle {err:.3e}, max-abs {np.max(np.abs(pre - q64)):.3e}")
+    assert err <= 1e-4
 
 
 def test_whiten_int16(gpu_lib, ref32, rec32):
