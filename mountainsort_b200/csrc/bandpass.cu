@@ -283,7 +283,7 @@ __device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geo
 
 // F1, forward columns of length L1 = RA * RB.
 template <int RA, int RB>
-__global__ void __launch_bounds__(256) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
+__global__ void __launch_bounds__(256, 2) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
                                                         Geom g, const float2* __restrict__ roots, int64_t unit0) {
     constexpr int n = RA * RB;
     extern __shared__ float4 smem_f4[];
@@ -693,7 +693,8 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     g.out_i16 = out_i16 ? 1 : 0;
     g.qscale = out_i16 ? 1.0 / bp.quantization_unit : 1.0;
     // signals per unit: up to 16, limited by the shared-memory budget
-    int log2G = 4;
+    // signals per unit: 16 by default (MS3GPU_BP_LOG2G lowers it, for tuning)
+    int log2G = (int)std::min<size_t>(4, env_size("MS3GPU_BP_LOG2G", 4));
     while (log2G > 0 && ((int64_t(1) << (log2G - 1)) >= g.P)) log2G--;
     while (log2G > 0 && (smem_bytes_for((int)plan->L1, 1 << log2G, plan->P1.twlen) > kSmemBudget ||
                          smem_bytes_for((int)plan->L2, 1 << log2G, plan->P2.twlen) > kSmemBudget))
@@ -708,7 +709,7 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     const int64_t nchunks = ceil_div(N, chunk);
     const int64_t units = nchunks * g.ngroups;
     const size_t unit_bytes = (size_t)L * G * sizeof(float2);
-    const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 96) << 20;
+    const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 512) << 20;
     int64_t per_batch = std::max<int64_t>(1, (int64_t)(budget / unit_bytes));
     per_batch = std::min<int64_t>(per_batch, std::min<int64_t>(units, 65535));
 
