@@ -101,6 +101,110 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
         for (int j = 0; j < 4; j++) dst[(ty * 4 + i) * kCT + tx * 4 + j] = accd[i][j];
 }
 
+// cov_partial8: the same partial tiles as cov_partial with 8 x 8 register
+// micro-tiles (64 threads per 64 x 64 tile), cp.async double buffering of
+// 16-timepoint stages, FP32 sums over 32 timepoints flushed to FP64.
+// Needs M % 4 == 0 and a 16-byte aligned X (16-byte asynchronous copies).
+constexpr int kTS = 16;  // timepoints per stage
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    const int n = valid ? 16 : 0;  // src-size 0: zero fill
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, int64_t M, int64_t N, int nb,
+                                                   int64_t tslice, double* __restrict__ partials) {
+    __shared__ __align__(16) float As[2][kTS][kCT];
+    __shared__ __align__(16) float Bs[2][kTS][kCT];
+    const int pair = blockIdx.x;
+    const int npairs = gridDim.x;
+    int bi = 0, rem = pair;
+    while (rem >= nb - bi) { rem -= nb - bi; bi++; }
+    const int bj = bi + rem;
+    const bool diag = (bi == bj);
+    const int64_t t_begin = (int64_t)blockIdx.y * tslice;
+    const int64_t t_end = min(N, t_begin + tslice);
+    const int nst = (int)((t_end - t_begin + kTS - 1) / kTS);
+    const int tid = threadIdx.x;
+    const int tx = tid & 7, ty = tid >> 3;
+
+    // each thread copies 4 float4 of A (and of B): stage rows tt = tid/16 + 4k, 16-byte column tid%16
+    auto issue = [&](int st, int buf) {
+        const int64_t tb = t_begin + (int64_t)st * kTS;
+        const int c4 = (tid & 15) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int tt = (tid >> 4) + 4 * k;
+            const int64_t t = tb + tt;
+            const int64_t ca = (int64_t)bi * kCT + c4, cb = (int64_t)bj * kCT + c4;
+            const bool tv = t < t_end;
+            cp_async16(&As[buf][tt][c4], X + (tv && ca < M ? t * M + ca : 0), tv && ca < M);
+            if (!diag) cp_async16(&Bs[buf][tt][c4], X + (tv && cb < M ? t * M + cb : 0), tv && cb < M);
+        }
+        cp_async_commit();
+    };
+
+    float acc[8][8];
+    double accd[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            acc[i][j] = 0.f;
+            accd[i][j] = 0.0;
+        }
+    if (nst > 0) issue(0, 0);
+    for (int st = 0; st < nst; st++) {
+        const int buf = st & 1;
+        if (st + 1 < nst) {
+            issue(st + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float(*A)[kCT] = As[buf];
+        const float(*B)[kCT] = diag ? As[buf] : Bs[buf];
+#pragma unroll
+        for (int tt = 0; tt < kTS; tt++) {
+            const float4 a0 = *reinterpret_cast<const float4*>(&A[tt][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&A[tt][32 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4*>(&B[tt][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&B[tt][32 + tx * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        __syncthreads();
+        if ((st & 1) || st + 1 == nst) {
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    accd[i][j] += (double)acc[i][j];
+                    acc[i][j] = 0.f;
+                }
+        }
+    }
+    double* dst = partials + ((size_t)blockIdx.y * npairs + pair) * (kCT * kCT);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int r = (i < 4) ? ty * 4 + i : 32 + ty * 4 + (i - 4);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = (j < 4) ? tx * 4 + j : 32 + tx * 4 + (j - 4);
+            dst[r * kCT + c] = accd[i][j];
+        }
+    }
+}
+
 __global__ void cov_reduce(const double* __restrict__ partials, int S, int npairs, int nb, int64_t M,
                            int64_t N, double* __restrict__ XXt) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,12 +460,16 @@ void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaSt
         MS3_CUDA(cudaMemsetAsync(XXt, 0, sizeof(double) * (size_t)(M * M), stream));
         return;
     }
-    const int64_t target = std::max<int64_t>(1, (int64_t)4 * num_sms() / npairs);
+    const bool vec = (M % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const int64_t target = std::max<int64_t>(1, (int64_t)(vec ? 8 : 4) * num_sms() / npairs);
     int64_t S = std::min<int64_t>(target, ceil_div(N, kTT));
     int64_t tslice = ceil_div(ceil_div(N, S), kTT) * kTT;
     S = ceil_div(N, tslice);
     DevBuf partials((size_t)S * npairs * kCT * kCT * sizeof(double), stream);
-    cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
+    if (vec)
+        cov_partial8<<<dim3(npairs, (unsigned)S), 64, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
+    else
+        cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
     MS3_LAUNCH_CHECK();
     const int64_t total = (int64_t)npairs * kCT * kCT;
     cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(partials.as<double>(), (int)S, npairs, nb,
