@@ -343,12 +343,12 @@ bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out) {
 }
 
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        bool drain, void* out, cudaStream_t stream) {
+                        bool drain, void* out, cudaStream_t stream, int* ext_err) {
     DevBuf wbuf(sizeof(float) * (size_t)(2 * M * M) + 256, stream);
     float* whi = wbuf.as<float>();
     float* wlo = whi + M * M;
-    int* err = reinterpret_cast<int*>(wlo + M * M);
-    MS3_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    int* err = ext_err ? ext_err : reinterpret_cast<int*>(wlo + M * M);
+    if (!ext_err) MS3_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
     w_split_tf32<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, whi, wlo);
     MS3_LAUNCH_CHECK();
     if (drain)
@@ -357,6 +357,7 @@ void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, d
         launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
     else
         launch_apply_tc<192, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+    if (ext_err) return;  // the caller checks the flag once for many calls
     int herr = 0;
     MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
     MS3_CUDA(cudaStreamSynchronize(stream));

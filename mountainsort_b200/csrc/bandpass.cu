@@ -57,6 +57,8 @@ struct Geom {
     int m_even;          // M even (pairs load as aligned float2)
     int log2G;           // signals per unit = 1 << log2G
     int ngroups;
+    int64_t c_begin;     // first window of this call
+    int64_t nwin;        // windows in this call
     int64_t L, L1, L2;
     int64_t chunk;
     int sub;
@@ -85,10 +87,9 @@ struct UnitIdx {
     int grp;
 };
 __device__ __forceinline__ UnitIdx unit_index(const Geom& g, int64_t unit) {
-    const int64_t nchunks = (g.N + g.chunk - 1) / g.chunk;
     UnitIdx u;
-    u.grp = (int)(unit / nchunks);
-    u.c = unit % nchunks;
+    u.grp = (int)(unit / g.nwin);
+    u.c = g.c_begin + unit % g.nwin;
     return u;
 }
 
@@ -660,7 +661,7 @@ int64_t bandpass_chunk_size(int64_t M, int64_t num_threads) {
 }
 
 void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, int64_t c_begin, int64_t c_end) {
     const int sub = bp.subsample_factor ? bp.subsample_factor : 1;
     if (sub < 1) throw_invalid("subsample_factor must be >= 1");
     const int64_t N2 = N / sub;
@@ -707,7 +708,12 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     const int G = 1 << log2G;
     g.ngroups = (int)ceil_div(g.P, G);
     const int64_t nchunks = ceil_div(N, chunk);
-    const int64_t units = nchunks * g.ngroups;
+    if (c_end < 0 || c_end > nchunks) c_end = nchunks;
+    if (c_begin < 0) c_begin = 0;
+    if (c_begin >= c_end) return;
+    g.c_begin = c_begin;
+    g.nwin = c_end - c_begin;
+    const int64_t units = g.nwin * g.ngroups;
     const size_t unit_bytes = (size_t)L * G * sizeof(float2);
     const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 512) << 20;
     int64_t per_batch = std::max<int64_t>(1, (int64_t)(budget / unit_bytes));
@@ -732,7 +738,7 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
         }
     }
     // Gaps between subsampled chunks stay zero, as in the preallocated file.
-    if (sub > 1 && chunk % sub != 0) {
+    if (sub > 1 && chunk % sub != 0 && c_begin == 0) {
         const size_t esz = out_i16 ? 2 : 4;
         MS3_CUDA(cudaMemsetAsync(out, 0, esz * (size_t)(M * N2), stream));
     }

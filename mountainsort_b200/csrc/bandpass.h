@@ -17,7 +17,10 @@ struct BandpassParams {
 int64_t bandpass_chunk_size(int64_t M, int64_t num_threads);
 
 // raw: device (N, M) float32 rows; out: device M x (N/sub), float32 or int16.
+// Filters the windows (chunks) [c_begin, c_end) of the recording (all by
+// default); window c reads raw rows [c*chunk - 60000, (c+1)*chunk + 60000)
+// and writes output rows [c*chunk, (c+1)*chunk) / sub.
 void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
-                     cudaStream_t stream);
+                     cudaStream_t stream, int64_t c_begin = 0, int64_t c_end = -1);
 
 }  // namespace ms3gpu

@@ -18,6 +18,7 @@
 #include "bandpass.h"
 #include "common.cuh"
 #include "ms3gpu.h"
+#include "pipeline.h"
 #include "whiten.h"
 
 namespace ms3gpu {
@@ -397,6 +398,13 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         const size_t pre_bytes = (q > 0 ? 2 : 4) * (size_t)(M * N);
         require(timeseries, "timeseries", in_bytes > 0);
         require(pre_out, "pre_out", pre_bytes > 0);
+        // host buffers: stream the recording through the device with overlapped copies
+        const char* nostream = std::getenv("MS3GPU_NO_STREAMING");
+        if (in_bytes > 0 && !is_device_ptr(timeseries) && !is_device_ptr(pre_out) &&
+            (!filt_out || !is_device_ptr(filt_out)) && !(nostream && nostream[0] == '1')) {
+            bandpass_whiten_streamed(timeseries, M, N, filt_out, pre_out, p, q, check_precision(wh->precision), s);
+            return;
+        }
         InView in;
         stage_in(in, timeseries, in_bytes, s);
         OutView filt;

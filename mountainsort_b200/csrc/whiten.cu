@@ -44,8 +44,8 @@ namespace {
 constexpr int kCT = 64;  // channel tile
 constexpr int kTT = 32;  // timepoints summed in FP32 before the FP64 add
 
-__global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, int64_t M, int64_t N, int nb,
-                                                   int64_t tslice, double* __restrict__ partials) {
+__global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, int64_t M, int64_t r0, int64_t N,
+                                                   int nb, int64_t tslice, double* __restrict__ partials) {
     __shared__ __align__(16) float As[kTT][kCT];
     __shared__ __align__(16) float Bs[kTT][kCT];
     const int pair = blockIdx.x;
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
     int bi = 0, rem = pair;
     while (rem >= nb - bi) { rem -= nb - bi; bi++; }
     const int bj = bi + rem;
-    const int64_t t_begin = (int64_t)blockIdx.y * tslice;
+    const int64_t t_begin = r0 + (int64_t)blockIdx.y * tslice;
     const int64_t t_end = min(N, t_begin + tslice);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     double accd[4][4];
@@ -116,8 +116,8 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, int64_t M, int64_t N, int nb,
-                                                   int64_t tslice, double* __restrict__ partials) {
+__global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, int64_t M, int64_t r0, int64_t N,
+                                                   int nb, int64_t tslice, double* __restrict__ partials) {
     __shared__ __align__(16) float As[2][kTS][kCT];
     __shared__ __align__(16) float Bs[2][kTS][kCT];
     const int pair = blockIdx.x;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, 
     while (rem >= nb - bi) { rem -= nb - bi; bi++; }
     const int bj = bi + rem;
     const bool diag = (bi == bj);
-    const int64_t t_begin = (int64_t)blockIdx.y * tslice;
+    const int64_t t_begin = r0 + (int64_t)blockIdx.y * tslice;
     const int64_t t_end = min(N, t_begin + tslice);
     const int nst = (int)((t_end - t_begin + kTS - 1) / kTS);
     const int tid = threadIdx.x;
@@ -452,29 +452,56 @@ int num_sms() {
 
 }  // namespace
 
-void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream) {
-    if (M <= 0) return;
-    const int nb = (int)ceil_div(M, kCT);
-    const int npairs = nb * (nb + 1) / 2;
-    if (N == 0) {
+CovPlan cov_plan(const float* X, int64_t M) {
+    CovPlan p;
+    p.nb = (int)ceil_div(M, kCT);
+    p.npairs = p.nb * (p.nb + 1) / 2;
+    p.vec = (M % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    return p;
+}
+
+int64_t cov_slices(const CovPlan& p, int64_t rows) {
+    if (rows <= 0) return 0;
+    const int64_t target = std::max<int64_t>(1, (int64_t)(p.vec ? 8 : 4) * num_sms() / p.npairs);
+    int64_t S = std::min<int64_t>(target, ceil_div(rows, kTT));
+    const int64_t tslice = ceil_div(ceil_div(rows, S), kTT) * kTT;
+    return ceil_div(rows, tslice);
+}
+
+size_t cov_partials_bytes(const CovPlan& p, int64_t slices) {
+    return (size_t)slices * p.npairs * kCT * kCT * sizeof(double);
+}
+
+void cov_partials(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPlan& p, double* partials,
+                  int64_t S, cudaStream_t stream) {
+    const int64_t rows = r1 - r0;
+    if (rows <= 0 || S <= 0) return;
+    const int64_t tslice = ceil_div(ceil_div(rows, S), kTT) * kTT;
+    if (p.vec)
+        cov_partial8<<<dim3(p.npairs, (unsigned)S), 64, 0, stream>>>(X, M, r0, r1, p.nb, tslice, partials);
+    else
+        cov_partial<<<dim3(p.npairs, (unsigned)S), 256, 0, stream>>>(X, M, r0, r1, p.nb, tslice, partials);
+    MS3_LAUNCH_CHECK();
+}
+
+void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, int64_t N, double* XXt,
+                cudaStream_t stream) {
+    if (S == 0) {
         MS3_CUDA(cudaMemsetAsync(XXt, 0, sizeof(double) * (size_t)(M * M), stream));
         return;
     }
-    const bool vec = (M % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-    const int64_t target = std::max<int64_t>(1, (int64_t)(vec ? 8 : 4) * num_sms() / npairs);
-    int64_t S = std::min<int64_t>(target, ceil_div(N, kTT));
-    int64_t tslice = ceil_div(ceil_div(N, S), kTT) * kTT;
-    S = ceil_div(N, tslice);
-    DevBuf partials((size_t)S * npairs * kCT * kCT * sizeof(double), stream);
-    if (vec)
-        cov_partial8<<<dim3(npairs, (unsigned)S), 64, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
-    else
-        cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, partials.as<double>());
+    const int64_t total = (int64_t)p.npairs * kCT * kCT;
+    cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(partials, (int)S, p.npairs, p.nb, M, N, XXt);
     MS3_LAUNCH_CHECK();
-    const int64_t total = (int64_t)npairs * kCT * kCT;
-    cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(partials.as<double>(), (int)S, npairs, nb,
-                                                                   M, N, XXt);
-    MS3_LAUNCH_CHECK();
+}
+
+void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream) {
+    if (M <= 0) return;
+    const CovPlan p = cov_plan(X, M);
+    const int64_t S = cov_slices(p, N);
+    DevBuf partials(cov_partials_bytes(p, S), stream);
+    cov_partials(X, M, 0, N, p, partials.as<double>(), S, stream);
+    cov_finish(partials.as<double>(), S, p, M, N, XXt, stream);
 }
 
 // ------------------------------------------------ covariance without allocation
@@ -535,7 +562,7 @@ void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt
     S = ceil_div(N, tslice);
     // Every partial tile the reduction reads is written by cov_partial in this
     // call, so nothing left in the array by an earlier call is ever used.
-    cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, N, nb, tslice, scratch);
+    cov_partial<<<dim3(npairs, (unsigned)S), 256, 0, stream>>>(X, M, 0, N, nb, tslice, scratch);
     MS3_LAUNCH_CHECK();
     const int64_t total = (int64_t)npairs * kCT * kCT;
     cov_reduce<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(scratch, (int)S, npairs, nb, M, N, XXt);
@@ -597,13 +624,13 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 }
 
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                            bool mixed, void* out, cudaStream_t stream) {
+                            bool mixed, void* out, cudaStream_t stream, int* err) {
     if (M <= 0 || N <= 0) return;
     // MS3GPU_APPLY_FFMA=1 selects the FP32 FMA kernel for the plain form
     const char* ffma = std::getenv("MS3GPU_APPLY_FFMA");
     const bool force_ffma = ffma && ffma[0] == '1';
     if (apply_tc_supported(X, M, N, out) && (mixed || !force_ffma)) {
-        apply_whitening_tc(X, M, N, W, quantization_unit, /*drain=*/!mixed, out, stream);
+        apply_whitening_tc(X, M, N, W, quantization_unit, /*drain=*/!mixed, out, stream, err);
         return;
     }
     DevBuf wt(sizeof(float) * (size_t)(M * M), stream);

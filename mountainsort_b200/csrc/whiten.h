@@ -10,6 +10,21 @@ namespace ms3gpu {
 // XXt (M x M doubles, column-major) = sum_t x_t x_t^T / (N-1 if N > 1).
 void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
 
+// The covariance in pieces, for callers that stream the rows in: partial
+// tiles of rows [r0, r1) go to `S` slices of a partials buffer; cov_finish
+// sums all slices written so far (fixed order) and divides by N-1.
+struct CovPlan {
+    int nb = 0, npairs = 0;
+    bool vec = false;
+};
+CovPlan cov_plan(const float* X, int64_t M);
+int64_t cov_slices(const CovPlan& p, int64_t rows);
+size_t cov_partials_bytes(const CovPlan& p, int64_t slices);
+void cov_partials(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPlan& p, double* partials,
+                  int64_t S, cudaStream_t stream);
+void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, int64_t N, double* XXt,
+                cudaStream_t stream);
+
 // The same covariance with its partial sums in a fixed 16 MiB device array
 // instead of allocated scratch (X and XXt must be device memory).
 void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
@@ -22,8 +37,11 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 // out = quantize(W^T x) per timepoint; out float32, or int16 when
 // quantization_unit > 0.  mixed: tensor-core 3-term TF32 (when the shapes
 // allow), else FP32 FMA.
+// err: optional device flag raised by a timed-out tensor-core pipeline; when
+// null the call checks it itself (synchronising the stream).
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W,
-                            double quantization_unit, bool mixed, void* out, cudaStream_t stream);
+                            double quantization_unit, bool mixed, void* out, cudaStream_t stream,
+                            int* err = nullptr);
 
 // Tensor-core (tcgen05, 3-term TF32) apply; apply_tc_supported tells whether
 // the shapes and alignment allow it.
@@ -31,6 +49,6 @@ bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out);
 // drain: per-K-block draining of the large products into round-to-nearest
 // FP32 sums (plain form); otherwise one FP32 TMEM accumulator (mixed form).
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        bool drain, void* out, cudaStream_t stream);
+                        bool drain, void* out, cudaStream_t stream, int* err = nullptr);
 
 }  // namespace ms3gpu
