@@ -13,18 +13,20 @@
 // are prepared once per call.  The representation error is ~2^-22 of each
 // term, the same order as the reference's own float accumulation.
 //
-// One CTA computes a 128 (timepoints) x BN (channels) output tile:
+// A persistent CTA per SM walks 128 (timepoints) x 128 (channels) output tiles:
 //   warp 0      TMA producer: X, Wt_hi, Wt_lo K-blocks of 32 into an
-//               S-stage ring (128-byte swizzle, the UMMA canonical layout)
+//               S-stage ring (128-byte swizzle, the UMMA canonical layout),
+//               streaming continuously across the CTA's tiles
 //   warp 1      TMEM allocation; one thread issues 3 MMAs per K=8 step and
 //               commits each stage back to the producer
-//   warps 4..7  convert X to X_lo per stage, then drain the accumulator
-//               (tcgen05.ld), round, store
+//   warps 2..3  convert X to X_lo per stage
+//   warps 4..7  drain the accumulators (tcgen05.ld), round, store
 // Every mbarrier wait is bounded (tc::mbar_wait); a timeout raises *err.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
@@ -48,8 +50,9 @@ struct TcCfg {
     static constexpr int kABytes = kTM * 128;  // 16 KB
     static constexpr int kBBytes = BN * 128;
     static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // X, X_lo, W_hi, W_lo
-    // DRAIN: two hi*hi accumulators (alternate K-blocks) + one for the small terms
-    static constexpr int kUsedCols = DRAIN ? 3 * BN : BN;
+    // two small-term accumulators (alternate tiles) and, with DRAIN, two hi*hi
+    // accumulators (alternate K-blocks)
+    static constexpr int kUsedCols = DRAIN ? 4 * BN : 2 * BN;
     static constexpr int kTmemCols = (kUsedCols <= 32) ? 32 : (kUsedCols <= 64) ? 64 : (kUsedCols <= 128) ? 128
                                      : (kUsedCols <= 256) ? 256 : 512;
     static constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
@@ -100,43 +103,54 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
     }
 }
 
+// Persistent: each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// with column blocks of one time tile adjacent in tile order, so the CTAs
+// running at any moment share their X tiles through L2.  The producer and
+// converter stream K-blocks continuously across tiles (a global K-block
+// counter g drives the stage ring), so the next tile's loads overlap the
+// current tile's last MMAs and epilogue.  The small-term accumulator
+// alternates between two TMEM buffers by tile parity.
+//
 // DRAIN = false (mixed form): all three products accumulate over the whole K
-// range in one FP32 TMEM accumulator.
+// range in the tile's small-term accumulator.
 // DRAIN = true (plain form): the tensor core's FP32 accumulation rounds
 // toward zero, so long accumulations of the large hi*hi terms drift.  Each
 // K-block's hi*hi products go to a fresh accumulator (two, alternating) that
 // the epilogue warps drain into round-to-nearest FP32 sums while the next
-// K-block runs; the small hi*lo + lo*hi terms keep one long-lived
-// accumulator (their rounding is ~2^-11 smaller).
+// K-block runs; the small hi*lo + lo*hi terms keep the tile's accumulator
+// (their rounding is ~2^-11 smaller).
 template <int BN, bool DRAIN>
 __global__ void __launch_bounds__(kThreadsTC, 1)
     apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
-                    const __grid_constant__ CUtensorMap tmWlo, int64_t M, int64_t N, int ncb, double qunit,
-                    void* __restrict__ out, int* __restrict__ err) {
+                    const __grid_constant__ CUtensorMap tmWlo, int64_t M, int64_t N, int ncb, int64_t ntiles,
+                    double qunit, void* __restrict__ out, int* __restrict__ err) {
     using C = TcCfg<BN, DRAIN>;
     constexpr int S = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * C::kStageBytes);
-    uint64_t* full = bars;               // TMA bytes landed
-    uint64_t* conv = bars + S;           // X_lo written
-    uint64_t* empty = bars + 2 * S;      // MMAs done reading the stage
-    uint64_t* done = bars + 3 * S;       // all MMAs done
-    uint64_t* acc_full = bars + 3 * S + 1;  // [2] hi*hi K-block accumulator ready (DRAIN)
-    uint64_t* acc_free = bars + 3 * S + 3;  // [2] accumulator drained (DRAIN)
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 5);
+    uint64_t* full = bars;                  // [S] TMA bytes landed
+    uint64_t* conv = bars + S;              // [S] X_lo written
+    uint64_t* empty = bars + 2 * S;         // [S] MMAs done reading the stage
+    uint64_t* acc_full = bars + 3 * S;      // [2] hi*hi K-block accumulator ready (DRAIN)
+    uint64_t* acc_free = bars + 3 * S + 2;  // [2] hi*hi accumulator drained (DRAIN)
+    uint64_t* tile_full = bars + 3 * S + 4;   // [2] all MMAs of a tile done
+    uint64_t* small_free = bars + 3 * S + 6;  // [2] tile accumulator read by the epilogue
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 8);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t tile = blockIdx.x / ncb;
-    const int cb = (int)(blockIdx.x % ncb);
-    const int64_t t0 = tile * kTM;
-    const int n0 = cb * BN;
     const int nkb = (int)((M + kKB - 1) / kKB);
+    const int64_t my_tiles = (blockIdx.x < ntiles) ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     auto stageA = [&](int s) { return smem + (size_t)s * C::kStageBytes; };
     auto stageAlo = [&](int s) { return smem + (size_t)s * C::kStageBytes + C::kABytes; };
     auto stageBhi = [&](int s) { return smem + (size_t)s * C::kStageBytes + 2 * C::kABytes; };
     auto stageBlo = [&](int s) { return smem + (size_t)s * C::kStageBytes + 2 * C::kABytes + C::kBBytes; };
+    auto tile_of = [&](int64_t i, int64_t& t0, int& n0) {
+        const int64_t tile = blockIdx.x + i * gridDim.x;
+        t0 = (tile / ncb) * kTM;
+        n0 = (int)(tile % ncb) * BN;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) {
@@ -144,10 +158,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             tc::mbar_init(&conv[s], 64);
             tc::mbar_init(&empty[s], 1);
         }
-        tc::mbar_init(done, 1);
         for (int b = 0; b < 2; b++) {
             tc::mbar_init(&acc_full[b], 1);
             tc::mbar_init(&acc_free[b], 128);
+            tc::mbar_init(&tile_full[b], 1);
+            tc::mbar_init(&small_free[b], 128);
         }
         tc::fence_mbar_init();
     }
@@ -156,65 +171,79 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t taddr = *tmem_slot;
-    const uint32_t acc_big[2] = {taddr, taddr + (uint32_t)BN};
-    const uint32_t acc_small = DRAIN ? taddr + 2u * BN : taddr;
+    // TMEM columns: small[0], small[1], then (DRAIN) big[0], big[1]
+    const uint32_t acc_small[2] = {taddr, taddr + (uint32_t)BN};
+    const uint32_t acc_big[2] = {taddr + 2u * BN, taddr + 3u * BN};
+    const int64_t total_kb = my_tiles * nkb;
 
     if (warp == 0) {
         if (lane == 0) {
-            int issued = 0;
-            for (int kb = 0; kb < nkb; kb++) {
-                const int s = kb % S;
-                if (kb >= S && !tc::mbar_wait(&empty[s], ((kb / S) - 1) & 1, err)) break;
+            int64_t issued = 0;
+            for (int64_t g = 0; g < total_kb; g++) {
+                const int s = (int)(g % S);
+                if (g >= S && !tc::mbar_wait(&empty[s], (uint32_t)(((g / S) - 1) & 1), err)) break;
+                int64_t t0;
+                int n0;
+                tile_of(g / nkb, t0, n0);
+                const int kb = (int)(g % nkb);
                 tc::mbar_expect_tx(&full[s], C::kABytes + 2 * C::kBBytes);
                 tc::tma_load_2d(stageA(s), &tmX, &full[s], kb * kKB, (int)t0);
                 tc::tma_load_2d(stageBhi(s), &tmWhi, &full[s], kb * kKB, n0);
                 tc::tma_load_2d(stageBlo(s), &tmWlo, &full[s], kb * kKB, n0);
-                issued = kb + 1;
+                issued = g + 1;
             }
             // no copy may still be landing in shared memory when the CTA exits
-            for (int kb = (issued > S ? issued - S : 0); kb < issued; kb++)
-                tc::mbar_wait(&full[kb % S], (kb / S) & 1, err);
+            for (int64_t g = (issued > S ? issued - S : 0); g < issued; g++)
+                tc::mbar_wait(&full[g % S], (uint32_t)((g / S) & 1), err);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             constexpr uint32_t idesc = tc::instr_desc(2u /*TF32*/, kTM, BN);
             bool ok = true;
-            for (int kb = 0; kb < nkb && ok; kb++) {
-                const int s = kb % S;
-                const int b = kb & 1;
-                ok = tc::mbar_wait(&full[s], (kb / S) & 1, err) && tc::mbar_wait(&conv[s], (kb / S) & 1, err);
-                if (ok && DRAIN && kb >= 2) ok = tc::mbar_wait(&acc_free[b], ((kb >> 1) - 1) & 1, err);
-                if (!ok) break;
-                tc::tc_fence_after();
-                const uint32_t a = tc::smem_u32(stageA(s)), al = tc::smem_u32(stageAlo(s));
-                const uint32_t bh = tc::smem_u32(stageBhi(s)), bl = tc::smem_u32(stageBlo(s));
+            for (int64_t i = 0; i < my_tiles && ok; i++) {
+                const int tp = (int)(i & 1);
+                if (i >= 2) ok = tc::mbar_wait(&small_free[tp], (uint32_t)(((i >> 1) - 1) & 1), err);
+                for (int kb = 0; kb < nkb && ok; kb++) {
+                    const int64_t g = i * nkb + kb;
+                    const int s = (int)(g % S);
+                    const int b = (int)(g & 1);
+                    ok = tc::mbar_wait(&full[s], (uint32_t)((g / S) & 1), err) &&
+                         tc::mbar_wait(&conv[s], (uint32_t)((g / S) & 1), err);
+                    if (ok && DRAIN && g >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)(((g >> 1) - 1) & 1), err);
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const uint32_t a = tc::smem_u32(stageA(s)), al = tc::smem_u32(stageAlo(s));
+                    const uint32_t bh = tc::smem_u32(stageBhi(s)), bl = tc::smem_u32(stageBlo(s));
 #pragma unroll
-                for (int ks = 0; ks < kKB / 8; ks++) {
-                    const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K inside the swizzle atom
-                    const uint64_t da = tc::smem_desc_k_sw128(a + off), dal = tc::smem_desc_k_sw128(al + off);
-                    const uint64_t dbh = tc::smem_desc_k_sw128(bh + off), dbl = tc::smem_desc_k_sw128(bl + off);
-                    if (DRAIN) {
-                        tc::mma_tf32(acc_big[b], da, dbh, idesc, ks != 0);
-                        tc::mma_tf32(acc_small, da, dbl, idesc, (kb | ks) != 0);
-                    } else {
-                        tc::mma_tf32(acc_small, da, dbh, idesc, (kb | ks) != 0);
-                        tc::mma_tf32(acc_small, da, dbl, idesc, 1);
+                    for (int ks = 0; ks < kKB / 8; ks++) {
+                        const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K inside the swizzle atom
+                        const uint64_t da = tc::smem_desc_k_sw128(a + off), dal = tc::smem_desc_k_sw128(al + off);
+                        const uint64_t dbh = tc::smem_desc_k_sw128(bh + off), dbl = tc::smem_desc_k_sw128(bl + off);
+                        if (DRAIN) {
+                            tc::mma_tf32(acc_big[b], da, dbh, idesc, ks != 0);
+                            tc::mma_tf32(acc_small[tp], da, dbl, idesc, (kb | ks) != 0);
+                        } else {
+                            tc::mma_tf32(acc_small[tp], da, dbh, idesc, (kb | ks) != 0);
+                            tc::mma_tf32(acc_small[tp], da, dbl, idesc, 1);
+                        }
+                        tc::mma_tf32(acc_small[tp], dal, dbh, idesc, 1);
                     }
-                    tc::mma_tf32(acc_small, dal, dbh, idesc, 1);
+                    tc::mma_commit(&empty[s]);
+                    if (DRAIN) tc::mma_commit(&acc_full[b]);
                 }
-                tc::mma_commit(&empty[s]);
-                if (DRAIN) tc::mma_commit(&acc_full[b]);
+                if (ok) tc::mma_commit(&tile_full[tp]);
             }
-            tc::mma_commit(done);
-            // no MMA may still be writing TMEM when it is freed
-            tc::mbar_wait(done, 0, err);
+            // no MMA may still be writing TMEM when it is freed: wait for the
+            // epilogue to have read the last two tiles' accumulators
+            for (int64_t i = (my_tiles > 2 ? my_tiles - 2 : 0); i < my_tiles && ok; i++)
+                ok = tc::mbar_wait(&small_free[i & 1], (uint32_t)((i >> 1) & 1), err);
         }
     } else if (warp < 4) {
         // warps 2-3: X_lo = rna_tf32(x - trunc_tf32(x)), same swizzled layout as X
         const int ct = threadIdx.x - 64;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % S;
-            if (!tc::mbar_wait(&full[s], (kb / S) & 1, err)) break;
+        for (int64_t g = 0; g < total_kb; g++) {
+            const int s = (int)(g % S);
+            if (!tc::mbar_wait(&full[s], (uint32_t)((g / S) & 1), err)) break;
             const uint32_t* src = reinterpret_cast<const uint32_t*>(stageA(s));
             uint32_t* dst = reinterpret_cast<uint32_t*>(stageAlo(s));
 #pragma unroll 8
@@ -231,43 +260,51 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         // warps 4-7: accumulator drain and epilogue; warp q reads TMEM lanes 32q..32q+31
         const int q = warp & 3;
         const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-        const int64_t t = t0 + q * 32 + lane;
         bool ok = true;
-        float sums[BN];
+        for (int64_t i = 0; i < my_tiles && ok; i++) {
+            const int tp = (int)(i & 1);
+            int64_t t0;
+            int n0;
+            tile_of(i, t0, n0);
+            const int64_t t = t0 + q * 32 + lane;
+            float sums[BN];
 #pragma unroll
-        for (int j = 0; j < BN; j++) sums[j] = 0.f;
-        if (DRAIN) {
-            for (int kb = 0; kb < nkb && ok; kb++) {
-                const int b = kb & 1;
-                ok = tc::mbar_wait(&acc_full[b], (kb >> 1) & 1, err);
-                if (!__all_sync(0xffffffffu, ok)) {
-                    ok = false;
-                    break;
+            for (int j = 0; j < BN; j++) sums[j] = 0.f;
+            if (DRAIN) {
+                for (int kb = 0; kb < nkb; kb++) {
+                    const int64_t g = i * nkb + kb;
+                    const int b = (int)(g & 1);
+                    ok = tc::mbar_wait(&acc_full[b], (uint32_t)((g >> 1) & 1), err);
+                    if (!__all_sync(0xffffffffu, ok)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+#pragma unroll
+                    for (int c0 = 0; c0 < BN; c0 += 32) {
+                        uint32_t r[32];
+                        tc::tmem_ld_32x32b_x32(acc_big[b] + lane_base + (uint32_t)c0, r);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) sums[c0 + j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
+                    }
+                    tc::tc_fence_before();
+                    tc::mbar_arrive(&acc_free[b]);
                 }
-                tc::tc_fence_after();
-#pragma unroll
-                for (int c0 = 0; c0 < BN; c0 += 32) {
-                    uint32_t r[32];
-                    tc::tmem_ld_32x32b_x32(acc_big[b] + lane_base + (uint32_t)c0, r);
-#pragma unroll
-                    for (int j = 0; j < 32; j++) sums[c0 + j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
-                }
-                tc::tc_fence_before();
-                tc::mbar_arrive(&acc_free[b]);
             }
-        }
-        if (ok) ok = tc::mbar_wait(done, 0, err);
-        if (__all_sync(0xffffffffu, ok)) {
+            if (ok) ok = tc::mbar_wait(&tile_full[tp], (uint32_t)((i >> 1) & 1), err);
+            if (!__all_sync(0xffffffffu, ok)) break;
             tc::tc_fence_after();
 #pragma unroll
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 uint32_t r[32];
-                tc::tmem_ld_32x32b_x32(acc_small + lane_base + (uint32_t)c0, r);
+                tc::tmem_ld_32x32b_x32(acc_small[tp] + lane_base + (uint32_t)c0, r);
                 float y[32];
 #pragma unroll
                 for (int j = 0; j < 32; j++) y[j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
                 if (t < N) store_row32(y, t, (int64_t)n0 + c0, M, qunit, out);
             }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&small_free[tp]);
         }
     }
     tc::tc_fence_before();
@@ -326,10 +363,13 @@ void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, con
     const CUtensorMap mh = make_map(whi, (uint64_t)M, (uint64_t)M, BN);
     const CUtensorMap ml = make_map(wlo, (uint64_t)M, (uint64_t)M, BN);
     const int ncb = (int)ceil_div(M, BN);
-    const int64_t blocks = ceil_div(N, kTM) * ncb;
-    if (blocks > 0x7fffffff) throw_unsupported("too many tiles for the tensor-core apply");
-    apply_tc_kernel<BN, DRAIN><<<(unsigned)blocks, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, qunit,
-                                                                                       out, err);
+    const int64_t ntiles = ceil_div(N, kTM) * ncb;
+    int dev = 0, nsm = 0;
+    MS3_CUDA(cudaGetDevice(&dev));
+    MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t grid = std::min<int64_t>(ntiles, nsm);  // one persistent CTA per SM
+    apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, ntiles,
+                                                                                     qunit, out, err);
     MS3_LAUNCH_CHECK();
 }
 
@@ -353,10 +393,8 @@ void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, d
     MS3_LAUNCH_CHECK();
     if (drain)
         launch_apply_tc<128, true>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
-    else if (M <= 128)
-        launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
     else
-        launch_apply_tc<192, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+        launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
     if (ext_err) return;  // the caller checks the flag once for many calls
     int herr = 0;
     MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
