@@ -55,21 +55,53 @@ struct TcCfg {
     static constexpr int kUsedCols = DRAIN ? 4 * BN : 2 * BN;
     static constexpr int kTmemCols = (kUsedCols <= 32) ? 32 : (kUsedCols <= 64) ? 64 : (kUsedCols <= 128) ? 128
                                      : (kUsedCols <= 256) ? 256 : 512;
-    static constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+    // output staging: two 32 x 32 float buffers per epilogue warp (128-byte swizzle)
+    static constexpr int kStagingBytes = 4 * 2 * 32 * 128;
+    static constexpr size_t kSmemBytes =
+        (size_t)kStages * kStageBytes + kStagingBytes + 1024 /*align*/ + 256 /*barriers*/;
 };
 
-__device__ __forceinline__ float quantize_1e4_tc(float x) {
-    const double xd = (double)x;
-    double t = __dadd_rn(__dmul_rn(xd, 10000.0), 0.5);
-    double f = floor(t);
-    if (t - f < 1e-6 || f + 1.0 - t < 1e-6) {
-        t = __dadd_rn(__ddiv_rn(xd, 0.0001), 0.5);
-        f = floor(t);
+// The reference's 1e-4 rounding, floor(x / 1e-4 + 0.5) * 1e-4 in double
+// (p_whiten.cpp:185-189), for 32 values in place.  x * 10000 stands in for
+// the division except within 1e-6 of a rounding boundary, where the two can
+// differ; those (rare) values are redone with the division in a second loop,
+// so the main loop has no branch and its 32 chains interleave.
+__device__ __forceinline__ void quantize_1e4_x32(float (&y)[32]) {
+#pragma unroll
+    for (int h = 0; h < 32; h += 16) {  // two halves keep the live registers down
+        uint32_t redo = 0;
+        float q[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const double t = __dadd_rn(__dmul_rn((double)y[h + j], 10000.0), 0.5);
+            const double f = floor(t);
+            redo |= (uint32_t)((t - f < 1e-6) | (f + 1.0 - t < 1e-6)) << j;
+            q[j] = (float)__dmul_rn(f, 0.0001);
+        }
+        if (redo) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                if ((redo >> j) & 1) {
+                    const double f = floor(__dadd_rn(__ddiv_rn((double)y[h + j], 0.0001), 0.5));
+                    q[j] = (float)__dmul_rn(f, 0.0001);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j++) y[h + j] = q[j];
     }
-    return (float)__dmul_rn(f, 0.0001);
 }
 
-// Rounds and stores 32 consecutive output channels of one timepoint.
+// x - trunc_tf32(x), rounded to TF32 (nearest, ties away from zero) and
+// returned as its 32-bit pattern: the same value cvt.rna.tf32.f32 gives.
+__device__ __forceinline__ uint32_t x_lo_tf32(uint32_t xb) {
+    const float lo = __uint_as_float(xb) - __uint_as_float(xb & 0xFFFFE000u);
+    return (__float_as_uint(lo) + 0x1000u) & 0xFFFFE000u;
+}
+
+// Stores 32 consecutive output channels of one timepoint, already rounded
+// to 1e-4; int16 output is scaled by the quantization unit as the reference
+// does ((int)(x / q + 0.5) truncated to 16 bits).
 __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int64_t nbase, int64_t M, double qunit,
                                             void* __restrict__ out) {
     if (qunit > 0) {
@@ -77,8 +109,7 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             if (nbase + j >= M) break;
-            const float q = quantize_1e4_tc(y[j]);
-            const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)q, qunit), 0.5));
+            const int32_t iv = x86_double_to_int32(__dadd_rn(__ddiv_rn((double)y[j], qunit), 0.5));
             o16[nbase + j] = x86_float_to_int16((float)iv);
         }
         return;
@@ -86,19 +117,12 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
     float* of = static_cast<float*>(out) + t * M + nbase;
     if (nbase + 32 <= M && ((reinterpret_cast<uintptr_t>(of) & 15) == 0)) {
 #pragma unroll
-        for (int j = 0; j < 32; j += 4) {
-            float4 v;
-            v.x = quantize_1e4_tc(y[j]);
-            v.y = quantize_1e4_tc(y[j + 1]);
-            v.z = quantize_1e4_tc(y[j + 2]);
-            v.w = quantize_1e4_tc(y[j + 3]);
-            *reinterpret_cast<float4*>(of + j) = v;
-        }
+        for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(of + j) = make_float4(y[j], y[j + 1], y[j + 2], y[j + 3]);
     } else {
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             if (nbase + j >= M) break;
-            of[j] = quantize_1e4_tc(y[j]);
+            of[j] = y[j];
         }
     }
 }
@@ -122,13 +146,15 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
 template <int BN, bool DRAIN>
 __global__ void __launch_bounds__(kThreadsTC, 1)
     apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
-                    const __grid_constant__ CUtensorMap tmWlo, int64_t M, int64_t N, int ncb, int64_t ntiles,
-                    double qunit, void* __restrict__ out, int* __restrict__ err) {
+                    const __grid_constant__ CUtensorMap tmWlo, const __grid_constant__ CUtensorMap tmOut, int out_tma,
+                    int64_t M, int64_t N, int ncb, int64_t ntiles, double qunit, void* __restrict__ out,
+                    int* __restrict__ err) {
     using C = TcCfg<BN, DRAIN>;
     constexpr int S = C::kStages;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * C::kStageBytes);
+    uint8_t* staging = smem + (size_t)S * C::kStageBytes;  // 1024-byte aligned
+    uint64_t* bars = reinterpret_cast<uint64_t*>(staging + C::kStagingBytes);
     uint64_t* full = bars;                  // [S] TMA bytes landed
     uint64_t* conv = bars + S;              // [S] X_lo written
     uint64_t* empty = bars + 2 * S;         // [S] MMAs done reading the stage
@@ -239,19 +265,26 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 ok = tc::mbar_wait(&small_free[i & 1], (uint32_t)((i >> 1) & 1), err);
         }
     } else if (warp < 4) {
-        // warps 2-3: X_lo = rna_tf32(x - trunc_tf32(x)), same swizzled layout as X
+        // warps 2-3: X_lo = rna_tf32(x - trunc_tf32(x)), same swizzled layout as X.
+        // x - trunc_tf32(x) is exact in FP32; its round-to-nearest-away TF32
+        // value is the integer round-half-up of its magnitude bits at bit 13
+        // (sign-magnitude encoding), which keeps the conversion on the
+        // full-rate integer pipe.
         const int ct = threadIdx.x - 64;
         for (int64_t g = 0; g < total_kb; g++) {
             const int s = (int)(g % S);
             if (!tc::mbar_wait(&full[s], (uint32_t)((g / S) & 1), err)) break;
-            const uint32_t* src = reinterpret_cast<const uint32_t*>(stageA(s));
-            uint32_t* dst = reinterpret_cast<uint32_t*>(stageAlo(s));
-#pragma unroll 8
-            for (int i = ct; i < kTM * kKB; i += 64) {
-                const uint32_t xb = src[i];
-                const float x = __uint_as_float(xb);
-                const float hi = __uint_as_float(xb & 0xFFFFE000u);
-                dst[i] = tc::cvt_rna_tf32(x - hi);
+            const uint4* src = reinterpret_cast<const uint4*>(stageA(s));
+            uint4* dst = reinterpret_cast<uint4*>(stageAlo(s));
+#pragma unroll 4
+            for (int i = ct; i < kTM * kKB / 4; i += 64) {
+                const uint4 xb = src[i];
+                uint4 r;
+                r.x = x_lo_tf32(xb.x);
+                r.y = x_lo_tf32(xb.y);
+                r.z = x_lo_tf32(xb.z);
+                r.w = x_lo_tf32(xb.w);
+                dst[i] = r;
             }
             tc::fence_proxy_async_smem();
             tc::mbar_arrive(&conv[s]);
@@ -260,6 +293,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         // warps 4-7: accumulator drain and epilogue; warp q reads TMEM lanes 32q..32q+31
         const int q = warp & 3;
         const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        int sbuf = 0;
         bool ok = true;
         for (int64_t i = 0; i < my_tiles && ok; i++) {
             const int tp = (int)(i & 1);
@@ -301,11 +335,33 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 float y[32];
 #pragma unroll
                 for (int j = 0; j < 32; j++) y[j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
-                if (t < N) store_row32(y, t, (int64_t)n0 + c0, M, qunit, out);
+                quantize_1e4_x32(y);
+                if (out_tma) {
+                    // this warp's 32 x 32 block through a swizzled staging buffer and
+                    // one TMA store (full 128-byte lines instead of 16-byte pieces)
+                    uint8_t* stg = staging + (size_t)(q * 2 + sbuf) * (32 * 128);
+                    if (lane == 0) tc::bulk_wait_group_read<1>();  // its previous store has read it
+                    __syncwarp();
+#pragma unroll
+                    for (int jj = 0; jj < 8; jj++) {
+                        const float4 v = make_float4(y[4 * jj], y[4 * jj + 1], y[4 * jj + 2], y[4 * jj + 3]);
+                        *reinterpret_cast<float4*>(stg + lane * 128 + ((jj ^ (lane & 7)) << 4)) = v;
+                    }
+                    tc::fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) {
+                        tc::tma_store_2d(&tmOut, stg, n0 + c0, (int)(t0 + q * 32));
+                        tc::bulk_commit_group();
+                    }
+                    sbuf ^= 1;
+                } else if (t < N) {
+                    store_row32(y, t, (int64_t)n0 + c0, M, qunit, out);
+                }
             }
             tc::tc_fence_before();
             tc::mbar_arrive(&small_free[tp]);
         }
+        if (out_tma && lane == 0) tc::bulk_wait_group<0>();  // stores complete before the CTA exits
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -362,14 +418,17 @@ void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, con
     const CUtensorMap mx = make_map(X, (uint64_t)M, (uint64_t)N, kTM);
     const CUtensorMap mh = make_map(whi, (uint64_t)M, (uint64_t)M, BN);
     const CUtensorMap ml = make_map(wlo, (uint64_t)M, (uint64_t)M, BN);
+    // float output goes out through TMA stores of 32 x 32 blocks
+    const int out_tma = (qunit <= 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
+    const CUtensorMap mo = out_tma ? make_map(out, (uint64_t)M, (uint64_t)N, 32) : mx;
     const int ncb = (int)ceil_div(M, BN);
     const int64_t ntiles = ceil_div(N, kTM) * ncb;
     int dev = 0, nsm = 0;
     MS3_CUDA(cudaGetDevice(&dev));
     MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(ntiles, nsm);  // one persistent CTA per SM
-    apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, M, N, ncb, ntiles,
-                                                                                     qunit, out, err);
+    apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, mo, out_tma, M, N, ncb,
+                                                                                     ntiles, qunit, out, err);
     MS3_LAUNCH_CHECK();
 }
 

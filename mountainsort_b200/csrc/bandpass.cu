@@ -41,6 +41,8 @@
 #include "common.cuh"
 #include "fft_block.cuh"
 #include "fft_reg.cuh"
+#include "ms3gpu.h"
+#include "tc_sm100.cuh"
 
 namespace ms3gpu {
 
@@ -242,18 +244,25 @@ __global__ void __launch_bounds__(kThreads) bp_cols_inverse(const float2* __rest
 }
 
 
-// Stores one filtered complex sample (two channels) at window index n of
-// window c, applying the trim to [60000, 60000 + chunk), the subsampling and
-// the int16 quantization of the reference (p_bandpass_filter.cpp:196-212).
-__device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geom& g, int64_t c, int64_t s,
-                                               int64_t n, float2 v) {
+// Stores one filtered complex sample (two channels) at window index n of a
+// window whose first kept sample lands at output timepoint ot_base =
+// (c * chunk) / sub, applying the trim to [60000, 60000 + chunk), the
+// subsampling and the int16 quantization of the reference
+// (p_bandpass_filter.cpp:196-212).  chunk < 2^31 (at most 2^30 / 24), so the
+// window arithmetic is 32-bit and needs no division when sub == 1.
+__device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geom& g, int64_t ot_base, int64_t s,
+                                               int n, float2 v) {
     if (s >= g.P) return;
-    const int64_t j = n - kOverlap;
-    if (j < 0 || j >= g.chunk) return;
-    if (g.sub != 1 && (j % g.sub)) return;
-    const int64_t jj = j / g.sub;
-    if (jj >= g.chunk / g.sub) return;
-    const int64_t ot = (c * g.chunk) / g.sub + jj;
+    const int j = n - (int)kOverlap;
+    if ((unsigned)j >= (unsigned)g.chunk) return;
+    int64_t ot = ot_base + j;
+    if (g.sub != 1) {
+        const int sub = g.sub;
+        if (j % sub) return;
+        const int jj = j / sub;
+        if (jj >= (int)g.chunk / sub) return;
+        ot = ot_base + jj;
+    }
     if (ot >= g.N2) return;
     const int64_t m0 = g.paired ? 2 * s : s;
     const bool has2 = g.paired && (m0 + 1 < g.M);
@@ -405,6 +414,149 @@ __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scra
     }
 }
 
+// F2, pipelined: the same arithmetic as bpr_rows_filter (bit-identical
+// results) in a persistent CTA per SM that walks rows r = blockIdx.x +
+// j * gridDim.x.  Each row (L2 x 16 complex values, 64000 bytes), its twiddle
+// row and its kernel row arrive by 1-D bulk copies into a ring of kF2Ring
+// shared-memory slots, issued kF2Ring rows ahead, so the global-load latency
+// overlaps the previous rows' arithmetic.  The three register passes then run
+// in place in the slot; the result goes straight back to the scratch row.
+constexpr int kF2Ring = 3;
+constexpr int kF2Threads = 416;  // 400 items in the outer passes, 320 in the middle one
+
+__device__ int g_bp_timeout;  // set when a pipeline wait gave up (checked by the host)
+
+template <int SA, int SB>
+struct F2Pipe {
+    static constexpr int n = SA * SB;
+    static constexpr int G = 16;
+    static constexpr int kRowBytes = n * G * 8;
+    static constexpr int kTwBytes = n * 8;
+    static constexpr int kKernBytes = n * 4;
+    static constexpr int kSlotBytes = kRowBytes + kTwBytes + kKernBytes;
+    static constexpr size_t kSmemBytes = (size_t)kF2Ring * kSlotBytes + n * 8 + kF2Ring * 8;
+    static_assert(kRowBytes % 16 == 0 && kTwBytes % 16 == 0 && kKernBytes % 16 == 0, "bulk copies need 16-byte sizes");
+    static_assert(SB * G <= kF2Threads && SA * G <= kF2Threads, "one item per thread");
+};
+
+template <int SA, int SB>
+__global__ void __launch_bounds__(kF2Threads, 1)
+    bpr_rows_filter_pipe(float2* __restrict__ scratch, Geom g, const float2* __restrict__ roots,
+                         const float2* __restrict__ twL, const float* __restrict__ kern, int64_t nrows) {
+    using P = F2Pipe<SA, SB>;
+    constexpr int n = P::n, G = P::G;
+    extern __shared__ float4 smem_f4[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(smem_f4);
+    float2* rt = reinterpret_cast<float2*>(smem + (size_t)kF2Ring * P::kSlotBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(rt + n);
+    const int64_t L1 = g.L1;
+    const int64_t mine = (blockIdx.x < nrows) ? (nrows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    auto slot_ptr = [&](int64_t j) { return smem + (size_t)(j % kF2Ring) * P::kSlotBytes; };
+    auto row_ptr = [&](int64_t j) {
+        const int64_t r = blockIdx.x + j * gridDim.x;
+        return scratch + (size_t)(r / L1) * (size_t)(g.L * G) + (size_t)(r % L1) * (n * G);
+    };
+    auto issue = [&](int64_t j) {
+        const int64_t k1 = (blockIdx.x + j * gridDim.x) % L1;
+        uint8_t* slot = slot_ptr(j);
+        uint64_t* bar = &full[j % kF2Ring];
+        tc::mbar_expect_tx(bar, P::kSlotBytes);
+        tc::bulk_load_1d(slot, row_ptr(j), P::kRowBytes, bar);
+        tc::bulk_load_1d(slot + P::kRowBytes, twL + k1 * n, P::kTwBytes, bar);
+        tc::bulk_load_1d(slot + P::kRowBytes + P::kTwBytes, kern + k1 * n, P::kKernBytes, bar);
+    };
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kF2Ring; s++) tc::mbar_init(&full[s], 1);
+        tc::fence_mbar_init();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int64_t j = 0; j < mine && j < kF2Ring; j++) issue(j);
+
+    const int t = threadIdx.x;
+    const bool outer = t < SB * G, middle = t < SA * G;
+    for (int64_t j = 0; j < mine; j++) {
+        // Re-derived every row through an opaque move: otherwise the compiler
+        // keeps the 40-odd loop-invariant root offsets q * i in registers
+        // across the row loop.
+        int i;
+        asm volatile("shr.b32 %0, %1, 4;" : "=r"(i) : "r"(t));
+        const int gi = t & (G - 1);
+        const bool landed = tc::mbar_wait(&full[j % kF2Ring], (uint32_t)((j / kF2Ring) & 1), &g_bp_timeout);
+        if (!__syncthreads_and(landed)) break;
+        uint8_t* slot = slot_ptr(j);
+        float2* buf = reinterpret_cast<float2*>(slot);
+        const float2* tw = reinterpret_cast<const float2*>(slot + P::kRowBytes);
+        const float* kr = reinterpret_cast<const float*>(slot + P::kRowBytes + P::kTwBytes);
+        // forward pass 1 (radix SA over items i < SB), in place
+        float2 u[SA];
+        if (outer) {
+#pragma unroll
+            for (int q = 0; q < SA; q++) {
+                const int n2 = i + q * SB;
+                u[q] = cmul(buf[n2 * G + gi], tw[n2]);
+            }
+            RegDft<SA, false>::run(u);
+        }
+        __syncthreads();
+        if (outer) {
+#pragma unroll
+            for (int q = 0; q < SA; q++) buf[(i * SA + q) * G + gi] = u[q];
+        }
+        __syncthreads();
+        // forward pass 2 (radix SB, items i < SA), kernel, inverse pass 1
+        float2 v[SB];
+        if (middle) {
+#pragma unroll
+            for (int q = 0; q < SB; q++) {
+                const float2 x = buf[(i + q * SA) * G + gi];
+                v[q] = (q == 0) ? x : cmul(x, rt[q * i]);
+            }
+            RegDft<SB, false>::run(v);
+#pragma unroll
+            for (int q = 0; q < SB; q++) {
+                const float kv = kr[i + q * SA];
+                v[q] = make_float2(v[q].x * kv, v[q].y * kv);
+            }
+            RegDft<SB, true>::run(v);
+        }
+        __syncthreads();
+        if (middle) {
+#pragma unroll
+            for (int q = 0; q < SB; q++) buf[(i * SB + q) * G + gi] = v[q];
+        }
+        __syncthreads();
+        // inverse pass 2 (radix SA, items i < SB), twiddle, store
+        if (outer) {
+            float2* row = row_ptr(j);
+#pragma unroll
+            for (int q = 0; q < SA; q++) {
+                const float2 x = buf[(i + q * SB) * G + gi];
+                if (q == 0) {
+                    u[q] = x;
+                } else {
+                    float2 w = rt[q * i];
+                    w.y = -w.y;
+                    u[q] = cmul(x, w);
+                }
+            }
+            RegDft<SA, true>::run(u);
+#pragma unroll
+            for (int q = 0; q < SA; q++) {
+                const int n2 = i + q * SB;
+                float2 w = tw[n2];
+                w.y = -w.y;
+                row[n2 * G + gi] = cmul(u[q], w);
+            }
+        }
+        // the slot's generic-proxy accesses are ordered before the next bulk copy into it
+        tc::fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && j + kF2Ring < mine) issue(j + kF2Ring);
+    }
+}
+
 // F3, inverse columns of length L1 = RA * RB (inverse order: radix RB, then
 // radix RA), trim / subsample / quantize, store.
 template <int RA, int RB>
@@ -419,6 +571,8 @@ __global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict
     const int n2 = blockIdx.x;
     const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
     const int64_t s0 = (int64_t)ui.grp * G;
+    const int64_t ot_base = (ui.c * g.chunk) / g.sub;
+    const int L2 = (int)g.L2;
     const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
     for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
         const int gi = it & (G - 1), i = it >> g.log2G;
@@ -447,8 +601,8 @@ __global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict
         RegDft<RA, true>::run(u);
 #pragma unroll
         for (int q = 0; q < RA; q++) {
-            const int64_t n1 = i + q * RB;
-            store_filtered(out, g, ui.c, s0 + gi, n1 * g.L2 + n2, u[q]);
+            const int n1 = i + q * RB;
+            store_filtered(out, g, ot_base, s0 + gi, n1 * L2 + n2, u[q]);
         }
     }
 }
@@ -734,6 +888,9 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             MS3_CUDA(cudaFuncSetAttribute(bpr_cols_inverse<kFastRA, kFastRB>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_rows_filter_pipe<kFastSA, kFastSB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)F2Pipe<kFastSA, kFastSB>::kSmemBytes));
             attrs_set[dev] = true;
         }
     }
@@ -741,6 +898,12 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     if (sub > 1 && chunk % sub != 0 && c_begin == 0) {
         const size_t esz = out_i16 ? 2 : 4;
         MS3_CUDA(cudaMemsetAsync(out, 0, esz * (size_t)(M * N2), stream));
+    }
+    int nsm = 0;
+    {
+        int dev = 0;
+        MS3_CUDA(cudaGetDevice(&dev));
+        MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     }
     DevBuf scratch((size_t)per_batch * unit_bytes, stream);
     const size_t fsm1 = ((size_t)plan->L1 * G + plan->L1) * sizeof(float2);
@@ -753,8 +916,15 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
         if (plan->fast) {
             bpr_cols_forward<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(raw, sc, g, plan->root1, u0);
             MS3_LAUNCH_CHECK();
-            bpr_rows_filter<kFastSA, kFastSB><<<g2, kFastSA * G, fsm2, stream>>>(sc, g, plan->root2, plan->twL,
-                                                                                 plan->kern);
+            if (G == F2Pipe<kFastSA, kFastSB>::G && reinterpret_cast<uintptr_t>(sc) % 16 == 0) {
+                const int64_t nrows = nb * plan->L1;
+                bpr_rows_filter_pipe<kFastSA, kFastSB>
+                    <<<(unsigned)std::min<int64_t>(nrows, nsm), kF2Threads, F2Pipe<kFastSA, kFastSB>::kSmemBytes,
+                       stream>>>(sc, g, plan->root2, plan->twL, plan->kern, nrows);
+            } else {
+                bpr_rows_filter<kFastSA, kFastSB><<<g2, kFastSA * G, fsm2, stream>>>(sc, g, plan->root2, plan->twL,
+                                                                                     plan->kern);
+            }
             MS3_LAUNCH_CHECK();
             bpr_cols_inverse<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0);
             MS3_LAUNCH_CHECK();
@@ -766,6 +936,18 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
             bp_cols_inverse<<<g1, kThreads, sm1, stream>>>(sc, out, g, plan->P1, plan->tw1, u0);
             MS3_LAUNCH_CHECK();
         }
+    }
+}
+
+void bandpass_check_timeout(cudaStream_t stream) {
+    int h = 0;
+    MS3_CUDA(cudaMemcpyFromSymbolAsync(&h, g_bp_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, stream));
+    MS3_CUDA(cudaStreamSynchronize(stream));
+    if (h) {
+        const int zero = 0;
+        MS3_CUDA(cudaMemcpyToSymbolAsync(g_bp_timeout, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream));
+        MS3_CUDA(cudaStreamSynchronize(stream));
+        throw Error(MS3GPU_ERR_CUDA, "bandpass: pipeline wait timed out");
     }
 }
 

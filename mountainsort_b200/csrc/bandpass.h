@@ -23,4 +23,9 @@ int64_t bandpass_chunk_size(int64_t M, int64_t num_threads);
 void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
                      cudaStream_t stream, int64_t c_begin = 0, int64_t c_end = -1);
 
+// Raises (and clears) the error a bandpass pipeline wait recorded when it gave
+// up; synchronizes `stream`.  Call once the bandpass work is ordered before
+// `stream`.
+void bandpass_check_timeout(cudaStream_t stream);
+
 }  // namespace ms3gpu

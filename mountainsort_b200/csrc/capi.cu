@@ -274,6 +274,7 @@ int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* 
         bandpass_device(static_cast<const float*>(in.ptr), M, N, out.ptr, p, s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        bandpass_check_timeout(s);
     });
 }
 
@@ -430,6 +431,7 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         if (filt_out) filt.finish(s);
         pre.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        bandpass_check_timeout(s);
     });
 }
 
