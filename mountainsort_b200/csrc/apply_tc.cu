@@ -42,20 +42,21 @@ namespace {
 
 constexpr int kTM = 128;       // timepoints per tile (MMA M)
 constexpr int kKB = 32;        // K elements per stage (one 128-byte row)
-constexpr int kThreadsTC = 256;
 
 template <int BN, bool DRAIN>
 struct TcCfg {
-    static constexpr int kStages = (BN <= 128) ? 3 : 2;
+    static constexpr int kStages = 3;
     static constexpr int kABytes = kTM * 128;  // 16 KB
     static constexpr int kBBytes = BN * 128;
     static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // X, X_lo, W_hi, W_lo
-    // two small-term accumulators (alternate tiles) and, with DRAIN, two hi*hi
-    // accumulators (alternate K-blocks)
+    // DRAIN: two per-K-block accumulators plus two tile sums (alternate
+    // tiles); mixed: two tile accumulators (alternate tiles)
     static constexpr int kUsedCols = DRAIN ? 4 * BN : 2 * BN;
     static constexpr int kTmemCols = (kUsedCols <= 32) ? 32 : (kUsedCols <= 64) ? 64 : (kUsedCols <= 128) ? 128
                                      : (kUsedCols <= 256) ? 256 : 512;
-    // output staging: two 32 x 32 float buffers per epilogue warp (128-byte swizzle)
+    // DRAIN adds a warpgroup that rounds and stores finished tiles
+    static constexpr int kThreads = DRAIN ? 384 : 256;
+    // output staging: two 32 x 32 float buffers per storing warp (128-byte swizzle)
     static constexpr int kStagingBytes = 4 * 2 * 32 * 128;
     static constexpr size_t kSmemBytes =
         (size_t)kStages * kStageBytes + kStagingBytes + 1024 /*align*/ + 256 /*barriers*/;
@@ -127,41 +128,70 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
     }
 }
 
+// Rounds 32 values of one timepoint to 1e-4 and writes them: float output
+// through the warp's swizzled staging buffer and one TMA store of the warp's
+// 32 x 32 block (full 128-byte lines), int16 output directly.
+__device__ __forceinline__ void emit_row32(float (&y)[32], int lane, uint8_t* staging_warp, int& sbuf,
+                                           const CUtensorMap* tmOut, int out_tma, int64_t t, int64_t trow0, int n,
+                                           int64_t M, int64_t N, double qunit, void* __restrict__ out) {
+    quantize_1e4_x32(y);
+    if (out_tma) {
+        uint8_t* stg = staging_warp + (size_t)sbuf * (32 * 128);
+        if (lane == 0) tc::bulk_wait_group_read<1>();  // its previous store has read it
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+            const float4 v = make_float4(y[4 * jj], y[4 * jj + 1], y[4 * jj + 2], y[4 * jj + 3]);
+            *reinterpret_cast<float4*>(stg + lane * 128 + ((jj ^ (lane & 7)) << 4)) = v;
+        }
+        tc::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            tc::tma_store_2d(tmOut, stg, n, (int)trow0);
+            tc::bulk_commit_group();
+        }
+        sbuf ^= 1;
+    } else if (t < N) {
+        store_row32(y, t, n, M, qunit, out);
+    }
+}
+
 // Persistent: each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
 // with column blocks of one time tile adjacent in tile order, so the CTAs
 // running at any moment share their X tiles through L2.  The producer and
 // converter stream K-blocks continuously across tiles (a global K-block
 // counter g drives the stage ring), so the next tile's loads overlap the
-// current tile's last MMAs and epilogue.  The small-term accumulator
-// alternates between two TMEM buffers by tile parity.
+// current tile's last MMAs and epilogue.
 //
 // DRAIN = false (mixed form): all three products accumulate over the whole K
-// range in the tile's small-term accumulator.
+// range in a tile accumulator; two alternate by tile parity so a tile's
+// epilogue (warps 4-7) overlaps the next tile's MMAs.
 // DRAIN = true (plain form): the tensor core's FP32 accumulation rounds
-// toward zero, so long accumulations of the large hi*hi terms drift.  Each
-// K-block's hi*hi products go to a fresh accumulator (two, alternating) that
-// the epilogue warps drain into round-to-nearest FP32 sums while the next
-// K-block runs; the small hi*lo + lo*hi terms keep the tile's accumulator
-// (their rounding is ~2^-11 smaller).
+// toward zero, so long accumulations drift.  Each K-block's three products go
+// to a fresh accumulator (two alternate) that warps 4-7 add into
+// round-to-nearest FP32 sums kept in TMEM while the next K-block runs; warps
+// 8-11 round and store a finished tile's sums during the next tile (the
+// sums alternate between two TMEM buffers by tile parity).
 template <int BN, bool DRAIN>
-__global__ void __launch_bounds__(kThreadsTC, 1)
+__global__ void __launch_bounds__(TcCfg<BN, DRAIN>::kThreads, 1)
     apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
                     const __grid_constant__ CUtensorMap tmWlo, const __grid_constant__ CUtensorMap tmOut, int out_tma,
                     int64_t M, int64_t N, int ncb, int64_t ntiles, double qunit, void* __restrict__ out,
                     int* __restrict__ err) {
     using C = TcCfg<BN, DRAIN>;
     constexpr int S = C::kStages;
+    constexpr int R = 2;  // accumulator ring (K-blocks when DRAIN, tiles when mixed)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* staging = smem + (size_t)S * C::kStageBytes;  // 1024-byte aligned
     uint64_t* bars = reinterpret_cast<uint64_t*>(staging + C::kStagingBytes);
-    uint64_t* full = bars;                  // [S] TMA bytes landed
-    uint64_t* conv = bars + S;              // [S] X_lo written
-    uint64_t* empty = bars + 2 * S;         // [S] MMAs done reading the stage
-    uint64_t* acc_full = bars + 3 * S;      // [2] hi*hi K-block accumulator ready (DRAIN)
-    uint64_t* acc_free = bars + 3 * S + 2;  // [2] hi*hi accumulator drained (DRAIN)
-    uint64_t* tile_full = bars + 3 * S + 4;   // [2] all MMAs of a tile done
-    uint64_t* small_free = bars + 3 * S + 6;  // [2] tile accumulator read by the epilogue
+    uint64_t* full = bars;                // [S] TMA bytes landed
+    uint64_t* conv = bars + S;            // [S] X_lo written
+    uint64_t* empty = bars + 2 * S;       // [S] MMAs done reading the stage
+    uint64_t* acc_full = bars + 3 * S;      // [2] accumulator complete (K-block, or tile when mixed)
+    uint64_t* acc_free = bars + 3 * S + 2;  // [2] accumulator read back
+    uint64_t* y_full = bars + 3 * S + 4;    // [2] DRAIN: a tile's sums complete in TMEM
+    uint64_t* y_free = bars + 3 * S + 6;    // [2] DRAIN: a tile's sums read by the storing warps
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 8);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -187,8 +217,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         for (int b = 0; b < 2; b++) {
             tc::mbar_init(&acc_full[b], 1);
             tc::mbar_init(&acc_free[b], 128);
-            tc::mbar_init(&tile_full[b], 1);
-            tc::mbar_init(&small_free[b], 128);
+            tc::mbar_init(&y_full[b], 128);
+            tc::mbar_init(&y_free[b], 128);
         }
         tc::fence_mbar_init();
     }
@@ -197,26 +227,33 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t taddr = *tmem_slot;
-    // TMEM columns: small[0], small[1], then (DRAIN) big[0], big[1]
-    const uint32_t acc_small[2] = {taddr, taddr + (uint32_t)BN};
-    const uint32_t acc_big[2] = {taddr + 2u * BN, taddr + 3u * BN};
+    // TMEM columns: accumulator b at b * BN; DRAIN keeps tile sums at (2 + tp) * BN
+    const uint32_t ysum[2] = {taddr + 2u * BN, taddr + 3u * BN};
     const int64_t total_kb = my_tiles * nkb;
 
     if (warp == 0) {
         if (lane == 0) {
-            int64_t issued = 0;
-            for (int64_t g = 0; g < total_kb; g++) {
-                const int s = (int)(g % S);
-                if (g >= S && !tc::mbar_wait(&empty[s], (uint32_t)(((g / S) - 1) & 1), err)) break;
-                int64_t t0;
-                int n0;
-                tile_of(g / nkb, t0, n0);
-                const int kb = (int)(g % nkb);
+            // indices advance incrementally: a 64-bit division here would sit on
+            // the stage ring's critical path
+            int64_t issued = 0, t0 = 0;
+            int n0 = 0, kb = 0, s = 0;
+            uint32_t phase = 0;  // parity of the previous use of stage s
+            if (my_tiles > 0) tile_of(0, t0, n0);
+            for (int64_t g = 0, i = 0; g < total_kb; g++) {
+                if (g >= S && !tc::mbar_wait(&empty[s], phase, err)) break;
                 tc::mbar_expect_tx(&full[s], C::kABytes + 2 * C::kBBytes);
                 tc::tma_load_2d(stageA(s), &tmX, &full[s], kb * kKB, (int)t0);
                 tc::tma_load_2d(stageBhi(s), &tmWhi, &full[s], kb * kKB, n0);
                 tc::tma_load_2d(stageBlo(s), &tmWlo, &full[s], kb * kKB, n0);
                 issued = g + 1;
+                if (++s == S) {
+                    s = 0;
+                    if (g + 1 > S) phase ^= 1;
+                }
+                if (++kb == nkb) {
+                    kb = 0;
+                    if (++i < my_tiles) tile_of(i, t0, n0);
+                }
             }
             // no copy may still be landing in shared memory when the CTA exits
             for (int64_t g = (issued > S ? issued - S : 0); g < issued; g++)
@@ -228,16 +265,18 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             bool ok = true;
             for (int64_t i = 0; i < my_tiles && ok; i++) {
                 const int tp = (int)(i & 1);
-                if (i >= 2) ok = tc::mbar_wait(&small_free[tp], (uint32_t)(((i >> 1) - 1) & 1), err);
+                // mixed: the tile accumulator must have been read back (tile i - 2)
+                if (!DRAIN && i >= 2) ok = tc::mbar_wait(&acc_free[tp], (uint32_t)(((i >> 1) - 1) & 1), err);
                 for (int kb = 0; kb < nkb && ok; kb++) {
                     const int64_t g = i * nkb + kb;
                     const int s = (int)(g % S);
-                    const int b = (int)(g & 1);
+                    const int b = DRAIN ? (int)(g % R) : tp;
                     ok = tc::mbar_wait(&full[s], (uint32_t)((g / S) & 1), err) &&
                          tc::mbar_wait(&conv[s], (uint32_t)((g / S) & 1), err);
-                    if (ok && DRAIN && g >= 2) ok = tc::mbar_wait(&acc_free[b], (uint32_t)(((g >> 1) - 1) & 1), err);
+                    if (ok && DRAIN && g >= R) ok = tc::mbar_wait(&acc_free[b], (uint32_t)(((g / R) - 1) & 1), err);
                     if (!ok) break;
                     tc::tc_fence_after();
+                    const uint32_t acc = taddr + (uint32_t)(b * BN);
                     const uint32_t a = tc::smem_u32(stageA(s)), al = tc::smem_u32(stageAlo(s));
                     const uint32_t bh = tc::smem_u32(stageBhi(s)), bl = tc::smem_u32(stageBlo(s));
 #pragma unroll
@@ -245,66 +284,67 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                         const uint32_t off = ks * 32;  // 8 TF32 = 32 bytes along K inside the swizzle atom
                         const uint64_t da = tc::smem_desc_k_sw128(a + off), dal = tc::smem_desc_k_sw128(al + off);
                         const uint64_t dbh = tc::smem_desc_k_sw128(bh + off), dbl = tc::smem_desc_k_sw128(bl + off);
-                        if (DRAIN) {
-                            tc::mma_tf32(acc_big[b], da, dbh, idesc, ks != 0);
-                            tc::mma_tf32(acc_small[tp], da, dbl, idesc, (kb | ks) != 0);
-                        } else {
-                            tc::mma_tf32(acc_small[tp], da, dbh, idesc, (kb | ks) != 0);
-                            tc::mma_tf32(acc_small[tp], da, dbl, idesc, 1);
-                        }
-                        tc::mma_tf32(acc_small[tp], dal, dbh, idesc, 1);
+                        tc::mma_tf32(acc, da, dbh, idesc, DRAIN ? (ks != 0) : ((kb | ks) != 0));
+                        tc::mma_tf32(acc, da, dbl, idesc, 1);
+                        tc::mma_tf32(acc, dal, dbh, idesc, 1);
                     }
                     tc::mma_commit(&empty[s]);
                     if (DRAIN) tc::mma_commit(&acc_full[b]);
                 }
-                if (ok) tc::mma_commit(&tile_full[tp]);
+                if (!DRAIN && ok) tc::mma_commit(&acc_full[tp]);
             }
-            // no MMA may still be writing TMEM when it is freed: wait for the
-            // epilogue to have read the last two tiles' accumulators
-            for (int64_t i = (my_tiles > 2 ? my_tiles - 2 : 0); i < my_tiles && ok; i++)
-                ok = tc::mbar_wait(&small_free[i & 1], (uint32_t)((i >> 1) & 1), err);
+            // mixed: no MMA may still be writing TMEM when it is freed
+            for (int64_t i = (my_tiles > 2 ? my_tiles - 2 : 0); !DRAIN && i < my_tiles && ok; i++)
+                ok = tc::mbar_wait(&acc_free[i & 1], (uint32_t)((i >> 1) & 1), err);
         }
     } else if (warp < 4) {
         // warps 2-3: X_lo = rna_tf32(x - trunc_tf32(x)), same swizzled layout as X.
         // x - trunc_tf32(x) is exact in FP32; its round-to-nearest-away TF32
         // value is the integer round-half-up of its magnitude bits at bit 13
         // (sign-magnitude encoding), which keeps the conversion on the
-        // full-rate integer pipe.
+        // full-rate integer pipe.  Eight 16-byte loads per thread are in flight at once.
         const int ct = threadIdx.x - 64;
         for (int64_t g = 0; g < total_kb; g++) {
             const int s = (int)(g % S);
             if (!tc::mbar_wait(&full[s], (uint32_t)((g / S) & 1), err)) break;
             const uint4* src = reinterpret_cast<const uint4*>(stageA(s));
             uint4* dst = reinterpret_cast<uint4*>(stageAlo(s));
-#pragma unroll 4
-            for (int i = ct; i < kTM * kKB / 4; i += 64) {
-                const uint4 xb = src[i];
-                uint4 r;
-                r.x = x_lo_tf32(xb.x);
-                r.y = x_lo_tf32(xb.y);
-                r.z = x_lo_tf32(xb.z);
-                r.w = x_lo_tf32(xb.w);
-                dst[i] = r;
+            constexpr int kPer = kTM * kKB / 4 / 64;
+#pragma unroll
+            for (int h = 0; h < kPer; h += 8) {
+                uint4 v[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) v[k] = src[ct + 64 * (h + k)];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    uint4 r;
+                    r.x = x_lo_tf32(v[k].x);
+                    r.y = x_lo_tf32(v[k].y);
+                    r.z = x_lo_tf32(v[k].z);
+                    r.w = x_lo_tf32(v[k].w);
+                    dst[ct + 64 * (h + k)] = r;
+                }
             }
             tc::fence_proxy_async_smem();
             tc::mbar_arrive(&conv[s]);
         }
-    } else {
-        // warps 4-7: accumulator drain and epilogue; warp q reads TMEM lanes 32q..32q+31
+    } else if (warp < 8) {
+        // warps 4-7; warp q reads TMEM lanes 32q..32q+31 (timepoints of the tile)
         const int q = warp & 3;
         const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        uint8_t* stg = staging + (size_t)q * 2 * (32 * 128);
         int sbuf = 0;
         bool ok = true;
         for (int64_t i = 0; i < my_tiles && ok; i++) {
-            const int tp = (int)(i & 1);
             int64_t t0;
             int n0;
             tile_of(i, t0, n0);
-            const int64_t t = t0 + q * 32 + lane;
-            float sums[BN];
-#pragma unroll
-            for (int j = 0; j < BN; j++) sums[j] = 0.f;
             if (DRAIN) {
+                // running round-to-nearest sums live in TMEM (ysum[tp]); the
+                // storing warps must have read this buffer's previous tile
+                const int tp = (int)(i & 1);
+                if (i >= 2) ok = tc::mbar_wait(&y_free[tp], (uint32_t)(((i >> 1) - 1) & 1), err);
+                if (!__all_sync(0xffffffffu, ok)) break;
                 for (int kb = 0; kb < nkb; kb++) {
                     const int64_t g = i * nkb + kb;
                     const int b = (int)(g & 1);
@@ -317,49 +357,70 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 #pragma unroll
                     for (int c0 = 0; c0 < BN; c0 += 32) {
                         uint32_t r[32];
-                        tc::tmem_ld_32x32b_x32(acc_big[b] + lane_base + (uint32_t)c0, r);
+                        tc::tmem_ld_32x32b_x32(taddr + (uint32_t)(b * BN) + lane_base + (uint32_t)c0, r);
+                        if (kb != 0) {
+                            uint32_t u[32];
+                            tc::tmem_ld_32x32b_x32(ysum[tp] + lane_base + (uint32_t)c0, u);
 #pragma unroll
-                        for (int j = 0; j < 32; j++) sums[c0 + j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
+                            for (int j = 0; j < 32; j++)
+                                r[j] = __float_as_uint(__fadd_rn(__uint_as_float(u[j]), __uint_as_float(r[j])));
+                        }
+                        tc::tmem_st_32x32b_x32(ysum[tp] + lane_base + (uint32_t)c0, r);
                     }
+                    tc::tmem_st_wait();
                     tc::tc_fence_before();
                     tc::mbar_arrive(&acc_free[b]);
                 }
+                if (!ok) break;
+                tc::mbar_arrive(&y_full[tp]);
+            } else {
+                const int tp = (int)(i & 1);
+                ok = tc::mbar_wait(&acc_full[tp], (uint32_t)((i >> 1) & 1), err);
+                if (!__all_sync(0xffffffffu, ok)) break;
+                tc::tc_fence_after();
+                const int64_t t = t0 + q * 32 + lane;
+#pragma unroll 1
+                for (int c0 = 0; c0 < BN; c0 += 32) {
+                    uint32_t r[32];
+                    tc::tmem_ld_32x32b_x32(taddr + (uint32_t)(tp * BN) + lane_base + (uint32_t)c0, r);
+                    float y[32];
+#pragma unroll
+                    for (int j = 0; j < 32; j++) y[j] = __uint_as_float(r[j]);
+                    emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, out);
+                }
+                tc::tc_fence_before();
+                tc::mbar_arrive(&acc_free[tp]);
             }
-            if (ok) ok = tc::mbar_wait(&tile_full[tp], (uint32_t)((i >> 1) & 1), err);
+        }
+        if (!DRAIN && out_tma && lane == 0) tc::bulk_wait_group<0>();  // stores complete before the CTA exits
+    } else if (DRAIN) {
+        // warps 8-11: round and store each tile's sums
+        const int q = warp & 3;
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        uint8_t* stg = staging + (size_t)q * 2 * (32 * 128);
+        int sbuf = 0;
+        for (int64_t i = 0; i < my_tiles; i++) {
+            int64_t t0;
+            int n0;
+            tile_of(i, t0, n0);
+            const int tp = (int)(i & 1);
+            const bool ok = tc::mbar_wait(&y_full[tp], (uint32_t)((i >> 1) & 1), err);
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::tc_fence_after();
-#pragma unroll
+            const int64_t t = t0 + q * 32 + lane;
+#pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 uint32_t r[32];
-                tc::tmem_ld_32x32b_x32(acc_small[tp] + lane_base + (uint32_t)c0, r);
+                tc::tmem_ld_32x32b_x32(ysum[tp] + lane_base + (uint32_t)c0, r);
+                if (c0 + 32 == BN) {  // every sum of the tile is read
+                    tc::tc_fence_before();
+                    tc::mbar_arrive(&y_free[tp]);
+                }
                 float y[32];
 #pragma unroll
-                for (int j = 0; j < 32; j++) y[j] = __fadd_rn(sums[c0 + j], __uint_as_float(r[j]));
-                quantize_1e4_x32(y);
-                if (out_tma) {
-                    // this warp's 32 x 32 block through a swizzled staging buffer and
-                    // one TMA store (full 128-byte lines instead of 16-byte pieces)
-                    uint8_t* stg = staging + (size_t)(q * 2 + sbuf) * (32 * 128);
-                    if (lane == 0) tc::bulk_wait_group_read<1>();  // its previous store has read it
-                    __syncwarp();
-#pragma unroll
-                    for (int jj = 0; jj < 8; jj++) {
-                        const float4 v = make_float4(y[4 * jj], y[4 * jj + 1], y[4 * jj + 2], y[4 * jj + 3]);
-                        *reinterpret_cast<float4*>(stg + lane * 128 + ((jj ^ (lane & 7)) << 4)) = v;
-                    }
-                    tc::fence_proxy_async_smem();
-                    __syncwarp();
-                    if (lane == 0) {
-                        tc::tma_store_2d(&tmOut, stg, n0 + c0, (int)(t0 + q * 32));
-                        tc::bulk_commit_group();
-                    }
-                    sbuf ^= 1;
-                } else if (t < N) {
-                    store_row32(y, t, (int64_t)n0 + c0, M, qunit, out);
-                }
+                for (int j = 0; j < 32; j++) y[j] = __uint_as_float(r[j]);
+                emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, out);
             }
-            tc::tc_fence_before();
-            tc::mbar_arrive(&small_free[tp]);
         }
         if (out_tma && lane == 0) tc::bulk_wait_group<0>();  // stores complete before the CTA exits
     }
@@ -427,7 +488,7 @@ void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, con
     MS3_CUDA(cudaGetDevice(&dev));
     MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(ntiles, nsm);  // one persistent CTA per SM
-    apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, kThreadsTC, C::kSmemBytes, stream>>>(mx, mh, ml, mo, out_tma, M, N, ncb,
+    apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, C::kThreads, C::kSmemBytes, stream>>>(mx, mh, ml, mo, out_tma, M, N, ncb,
                                                                                      ntiles, qunit, out, err);
     MS3_LAUNCH_CHECK();
 }
