@@ -41,13 +41,14 @@ namespace {
 
 // ------------------------------------------------------------ covariance
 
-constexpr int kCT = 64;  // channel tile
-constexpr int kTT = 32;  // timepoints summed in FP32 before the FP64 add
+constexpr int kCT = 64;   // channel tile
+constexpr int kTT = 32;  // timepoints summed in FP32 before the FP64 add (slice granularity)
+constexpr int kTG = 32;   // timepoints per shared-memory stage of cov_partial
 
 __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, int64_t M, int64_t r0, int64_t N,
                                                    int nb, int64_t tslice, double* __restrict__ partials) {
-    __shared__ __align__(16) float As[kTT][kCT];
-    __shared__ __align__(16) float Bs[kTT][kCT];
+    __shared__ __align__(16) float As[kTG][kCT];
+    __shared__ __align__(16) float Bs[kTG][kCT];
     const int pair = blockIdx.x;
     const int npairs = gridDim.x;
     int bi = 0, rem = pair;
@@ -57,13 +58,17 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
     const int64_t t_end = min(N, t_begin + tslice);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     double accd[4][4];
+    float acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) accd[i][j] = 0.0;
+        for (int j = 0; j < 4; j++) {
+            accd[i][j] = 0.0;
+            acc[i][j] = 0.f;
+        }
 
-    for (int64_t t0 = t_begin; t0 < t_end; t0 += kTT) {
-        for (int e = threadIdx.x; e < kTT * kCT; e += blockDim.x) {
+    for (int64_t t0 = t_begin; t0 < t_end; t0 += kTG) {
+        for (int e = threadIdx.x; e < kTG * kCT; e += blockDim.x) {
             const int tt = e / kCT, c = e % kCT;
             const int64_t t = t0 + tt;
             const int64_t ma = (int64_t)bi * kCT + c, mb = (int64_t)bj * kCT + c;
@@ -72,13 +77,8 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
             Bs[tt][c] = (tv && mb < M) ? X[t * M + mb] : 0.f;
         }
         __syncthreads();
-        float acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
 #pragma unroll 8
-        for (int tt = 0; tt < kTT; tt++) {
+        for (int tt = 0; tt < kTG; tt++) {
             const float4 a = *reinterpret_cast<const float4*>(&As[tt][ty * 4]);
             const float4 b = *reinterpret_cast<const float4*>(&Bs[tt][tx * 4]);
             const float av[4] = {a.x, a.y, a.z, a.w};
@@ -88,10 +88,16 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
 #pragma unroll
                 for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
         }
+        // flush the FP32 run every kTT timepoints of the slice
+        if (((t0 - t_begin + kTG) % kTT) == 0 || t0 + kTG >= t_end) {
 #pragma unroll
-        for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) accd[i][j] += (double)acc[i][j];
+                for (int j = 0; j < 4; j++) {
+                    accd[i][j] += (double)acc[i][j];
+                    acc[i][j] = 0.f;
+                }
+        }
         __syncthreads();
     }
     double* dst = partials + ((size_t)blockIdx.y * npairs + pair) * (kCT * kCT);
@@ -102,10 +108,14 @@ __global__ void __launch_bounds__(256) cov_partial(const float* __restrict__ X, 
 }
 
 // cov_partial8: the same partial tiles as cov_partial with 8 x 8 register
-// micro-tiles (64 threads per 64 x 64 tile), cp.async double buffering of
-// 16-timepoint stages, FP32 sums over 32 timepoints flushed to FP64.
-// Needs M % 4 == 0 and a 16-byte aligned X (16-byte asynchronous copies).
-constexpr int kTS = 16;  // timepoints per stage
+// micro-tiles (64 threads per 64 x 64 tile), a 3-deep cp.async ring of
+// 16-timepoint stages, and packed FP32 FMAs (fma.rn.f32x2: two independent
+// round-to-nearest FMAs per instruction, the same values as two fmaf calls),
+// which halve the issue slots of the inner product.  FP32 runs of kTT
+// timepoints are flushed to FP64, as in cov_partial, so both kernels produce
+// the same FP32 partial sums.  Needs M % 4 == 0 and a 16-byte aligned X.
+constexpr int kTS = 16;     // timepoints per stage
+constexpr int kStages8 = 3;
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool valid) {
     const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
@@ -116,10 +126,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// (a, a) as a packed FP32 pair
+__device__ __forceinline__ uint64_t dup_f32x2(float a) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+    return r;
+}
+// d = a * b + d on both halves of packed FP32 pairs
+__device__ __forceinline__ void fma_f32x2(uint64_t& d, uint64_t a, uint64_t b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+
 __global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, int64_t M, int64_t r0, int64_t N,
                                                    int nb, int64_t tslice, double* __restrict__ partials) {
-    __shared__ __align__(16) float As[2][kTS][kCT];
-    __shared__ __align__(16) float Bs[2][kTS][kCT];
+    __shared__ __align__(16) float As[kStages8][kTS][kCT];
+    __shared__ __align__(16) float Bs[kStages8][kTS][kCT];
     const int pair = blockIdx.x;
     const int npairs = gridDim.x;
     int bi = 0, rem = pair;
@@ -145,27 +166,27 @@ __global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, 
             cp_async16(&As[buf][tt][c4], X + (tv && ca < M ? t * M + ca : 0), tv && ca < M);
             if (!diag) cp_async16(&Bs[buf][tt][c4], X + (tv && cb < M ? t * M + cb : 0), tv && cb < M);
         }
-        cp_async_commit();
     };
 
-    float acc[8][8];
+    uint64_t acc[8][4];  // packed pairs: columns (2j, 2j + 1) of row i
     double accd[8][8];
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 8; i++) {
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            acc[i][j] = 0.f;
-            accd[i][j] = 0.0;
-        }
-    if (nst > 0) issue(0, 0);
+        for (int j = 0; j < 4; j++) acc[i][j] = 0ull;
+#pragma unroll
+        for (int j = 0; j < 8; j++) accd[i][j] = 0.0;
+    }
+#pragma unroll
+    for (int p = 0; p < kStages8 - 1; p++) {
+        if (p < nst) issue(p, p);
+        cp_async_commit();
+    }
     for (int st = 0; st < nst; st++) {
-        const int buf = st & 1;
-        if (st + 1 < nst) {
-            issue(st + 1, buf ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        const int buf = st % kStages8;
+        if (st + kStages8 - 1 < nst) issue(st + kStages8 - 1, (st + kStages8 - 1) % kStages8);
+        cp_async_commit();
+        cp_async_wait<kStages8 - 1>();
         __syncthreads();
         const float(*A)[kCT] = As[buf];
         const float(*B)[kCT] = diag ? As[buf] : Bs[buf];
@@ -173,23 +194,26 @@ __global__ void __launch_bounds__(64) cov_partial8(const float* __restrict__ X, 
         for (int tt = 0; tt < kTS; tt++) {
             const float4 a0 = *reinterpret_cast<const float4*>(&A[tt][ty * 4]);
             const float4 a1 = *reinterpret_cast<const float4*>(&A[tt][32 + ty * 4]);
-            const float4 b0 = *reinterpret_cast<const float4*>(&B[tt][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4*>(&B[tt][32 + tx * 4]);
+            const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(&B[tt][tx * 4]);
+            const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(&B[tt][32 + tx * 4]);
             const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const uint64_t bv[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
-            for (int i = 0; i < 8; i++)
+            for (int i = 0; i < 8; i++) {
+                const uint64_t ai = dup_f32x2(av[i]);
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                for (int j = 0; j < 4; j++) fma_f32x2(acc[i][j], ai, bv[j]);
+            }
         }
         __syncthreads();
-        if ((st & 1) || st + 1 == nst) {
+        if ((((st + 1) * kTS) % kTT) == 0 || st + 1 == nst) {
 #pragma unroll
             for (int i = 0; i < 8; i++)
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    accd[i][j] += (double)acc[i][j];
-                    acc[i][j] = 0.f;
+                for (int j = 0; j < 4; j++) {
+                    accd[i][2 * j] += (double)__uint_as_float((uint32_t)acc[i][j]);
+                    accd[i][2 * j + 1] += (double)__uint_as_float((uint32_t)(acc[i][j] >> 32));
+                    acc[i][j] = 0ull;
                 }
         }
     }
