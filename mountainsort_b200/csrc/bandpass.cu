@@ -305,11 +305,20 @@ __global__ void __launch_bounds__(256, 2) bpr_cols_forward(const float* __restri
     const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
     const int64_t t0 = ui.c * g.chunk - kOverlap + n2;
     const int64_t s0 = (int64_t)ui.grp * G;
+    // interior window of whole channel pairs: plain strided loads, no checks
+    const bool interior = g.paired && g.m_even && s0 + G <= g.P && t0 >= 0 && t0 + (int64_t)(n - 1) * g.L2 < g.N;
     for (int it = threadIdx.x; it < (RB << g.log2G); it += blockDim.x) {
         const int gi = it & (G - 1), i = it >> g.log2G;
         float2 u[RA];
+        if (interior) {
+            const float2* p = reinterpret_cast<const float2*>(raw + (t0 + (int64_t)i * g.L2) * g.M) + (s0 + gi);
+            const int64_t step = (int64_t)RB * g.L2 * (g.M / 2);  // float2 per RB window rows
 #pragma unroll
-        for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * g.L2, s0 + gi);
+            for (int q = 0; q < RA; q++) u[q] = __ldg(p + q * step);
+        } else {
+#pragma unroll
+            for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * g.L2, s0 + gi);
+        }
         RegDft<RA, false>::run(u);
 #pragma unroll
         for (int q = 0; q < RA; q++) buf[((i * RA + q) << g.log2G) + gi] = u[q];
@@ -560,8 +569,9 @@ __global__ void __launch_bounds__(kF2Threads, 1)
 // F3, inverse columns of length L1 = RA * RB (inverse order: radix RB, then
 // radix RA), trim / subsample / quantize, store.
 template <int RA, int RB>
-__global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict__ scratch, void* __restrict__ out,
-                                                        Geom g, const float2* __restrict__ roots, int64_t unit0) {
+__global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restrict__ scratch, void* __restrict__ out,
+                                                        Geom g, const float2* __restrict__ roots, int64_t unit0,
+                                                        int direct_ok) {
     constexpr int n = RA * RB;
     extern __shared__ float4 smem_f4[];
     float2* buf = reinterpret_cast<float2*>(smem_f4);
@@ -573,6 +583,13 @@ __global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict
     const int64_t s0 = (int64_t)ui.grp * G;
     const int64_t ot_base = (ui.c * g.chunk) / g.sub;
     const int L2 = (int)g.L2;
+    // float output of whole channel pairs, no subsampling, the whole chunk
+    // inside the output: the kept window rows n1 in [60000 / L2, (60000 +
+    // chunk) / L2) are exactly q in [kQ0, kQ1) for every item i < RB (checked
+    // on the host for this geometry), so plain strided stores of those q only
+    constexpr int kQ0 = 4, kQ1 = 12;
+    const bool direct = direct_ok && g.sub == 1 && !g.out_i16 && g.paired && g.m_even && s0 + G <= g.P &&
+                        (ui.c + 1) * g.chunk <= g.N2;
     const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
     for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
         const int gi = it & (G - 1), i = it >> g.log2G;
@@ -599,10 +616,22 @@ __global__ void __launch_bounds__(256) bpr_cols_inverse(const float2* __restrict
             }
         }
         RegDft<RA, true>::run(u);
+        if (direct) {
+            // kept window rows n1 in [kOverlap / L2, (kOverlap + chunk) / L2) are
+            // exactly q in [q0, q1) for every item i < RB
+            float2* o = reinterpret_cast<float2*>(static_cast<float*>(out) +
+                                                  (ot_base + (int64_t)i * L2 + n2 - kOverlap + (int64_t)kQ0 * RB * L2) *
+                                                      g.M) +
+                        (s0 + gi);
+            const int64_t step = (int64_t)RB * L2 * (g.M / 2);
 #pragma unroll
-        for (int q = 0; q < RA; q++) {
-            const int n1 = i + q * RB;
-            store_filtered(out, g, ot_base, s0 + gi, n1 * L2 + n2, u[q]);
+            for (int q = kQ0; q < kQ1; q++) o[(q - kQ0) * step] = u[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < RA; q++) {
+                const int n1 = i + q * RB;
+                store_filtered(out, g, ot_base, s0 + gi, n1 * L2 + n2, u[q]);
+            }
         }
     }
 }
@@ -908,6 +937,10 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     DevBuf scratch((size_t)per_batch * unit_bytes, stream);
     const size_t fsm1 = ((size_t)plan->L1 * G + plan->L1) * sizeof(float2);
     const size_t fsm2 = ((size_t)plan->L2 * G + plan->L2) * sizeof(float2);
+    // the register-pass inverse stores kept rows q in [4, 12) of each 16-point
+    // column transform directly when the trim falls on those row boundaries
+    const int direct_ok = (plan->fast && kOverlap == 4 * kFastRB * plan->L2 &&
+                           chunk == 8 * kFastRB * plan->L2) ? 1 : 0;
     for (int64_t u0 = 0; u0 < units; u0 += per_batch) {
         const int64_t nb = std::min<int64_t>(per_batch, units - u0);
         dim3 g1((unsigned)plan->L2, (unsigned)nb);
@@ -926,7 +959,7 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
                                                                                      plan->kern);
             }
             MS3_LAUNCH_CHECK();
-            bpr_cols_inverse<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0);
+            bpr_cols_inverse<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0, direct_ok);
             MS3_LAUNCH_CHECK();
         } else {
             bp_cols_forward<<<g1, kThreads, sm1, stream>>>(raw, sc, g, plan->P1, plan->tw1, u0);
