@@ -293,7 +293,7 @@ __device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geo
 
 // F1, forward columns of length L1 = RA * RB.
 template <int RA, int RB>
-__global__ void __launch_bounds__(256, 2) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
+__global__ void __launch_bounds__(256, 3) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
                                                         Geom g, const float2* __restrict__ roots, int64_t unit0) {
     constexpr int n = RA * RB;
     extern __shared__ float4 smem_f4[];
@@ -334,8 +334,10 @@ __global__ void __launch_bounds__(256, 2) bpr_cols_forward(const float* __restri
             u[q] = (q == 0) ? v : cmul(v, rt[q * i]);
         }
         RegDft<RB, false>::run(u);
+        float2* o = slab + (((size_t)i * g.L2 + n2) << g.log2G) + gi;
+        const size_t step = ((size_t)RA * g.L2) << g.log2G;
 #pragma unroll
-        for (int q = 0; q < RB; q++) slab[(((size_t)(i + q * RA) * g.L2 + n2) << g.log2G) + gi] = u[q];
+        for (int q = 0; q < RB; q++) o[q * step] = u[q];
     }
 }
 
@@ -594,8 +596,10 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restr
     for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
         const int gi = it & (G - 1), i = it >> g.log2G;
         float2 u[RB];
+        const float2* p = slab + (((size_t)i * g.L2 + n2) << g.log2G) + gi;
+        const size_t step = ((size_t)RA * g.L2) << g.log2G;
 #pragma unroll
-        for (int q = 0; q < RB; q++) u[q] = slab[(((size_t)(i + q * RA) * g.L2 + n2) << g.log2G) + gi];
+        for (int q = 0; q < RB; q++) u[q] = p[q * step];
         RegDft<RB, true>::run(u);
 #pragma unroll
         for (int q = 0; q < RB; q++) buf[((i * RB + q) << g.log2G) + gi] = u[q];
