@@ -172,6 +172,25 @@ MS3GPU_API int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M,
                                   double quantization_unit, int32_t precision, void* timeseries_out,
                                   void* stream);
 
+/* ms3.compute_whitening_matrix (p_whiten.cpp:208-298): XXt over the
+ * recordings of timeseries_list concatenated in time (n_inputs arrays of M
+ * channels; recording i has N_list[i] timepoints), restricted to `channels`
+ * (n_channels 1-based channel numbers, the processor's "channels" parameter;
+ * NULL / 0 = all M), divided by (sum of N_list) - 1 when that is above 1,
+ * then the whitening matrix of ms3gpu_whitening_matrix.  W_out: M2 x M2
+ * doubles (M2 = n_channels, or M), column-major.  Channel numbers outside
+ * [1, M] are MS3GPU_ERR_INVALID (the reference indexes out of range). */
+MS3GPU_API int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const int64_t* N_list,
+                                               int32_t n_inputs, int64_t M, const int32_t* channels,
+                                               int32_t n_channels, double* W_out, void* stream);
+
+/* ms3.whiten_clips (p_whiten.cpp:300-345): for every timepoint of every clip
+ * of an M x T x L float32 array, out(m1, t, l) = sum_m2 x(m2, t, l)
+ * W[m1*M + m2] -- the apply of ms3gpu_apply_whitening_matrix without the 1e-4
+ * rounding -- then int16 (int)(y/q + 0.5) when quantization_unit > 0. */
+MS3GPU_API int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* W,
+                                   double quantization_unit, int32_t precision, void* clips_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -186,6 +186,45 @@ def apply_whitening_matrix(X, W, quantization_unit=0.0, out=None, stream=None, p
     return out
 
 
+def compute_whitening_matrix(X_list, channels=None, stream=None):
+    """ms3.compute_whitening_matrix (p_whiten.cpp:208-298): the whitening
+    matrix of the recordings in X_list -- (N_i, M) arrays, concatenated in
+    time -- restricted to `channels` (1-based channel numbers) when given."""
+    L = _lib.load()
+    if not X_list:
+        raise ValueError("X_list is empty")
+    arrs = [_as_f32_rows(X) for X in X_list]
+    M = arrs[0].shape[1]
+    if any(a.ndim != 2 or a.shape[1] != M for a in arrs):
+        raise ValueError("all recordings need the same number of channels")
+    ptrs = (ctypes.c_void_p * len(arrs))(*[_ptr(a) for a in arrs])
+    Ns = (ctypes.c_int64 * len(arrs))(*[a.shape[0] for a in arrs])
+    ch = np.ascontiguousarray(channels if channels is not None else [], dtype=np.int32)
+    M2 = len(ch) if len(ch) else M
+    W = _empty_like(arrs[0], (M2, M2), np.float64)
+    check(L.ms3gpu_compute_whitening_matrix(ctypes.cast(ptrs, ctypes.c_void_p), ctypes.cast(Ns, ctypes.c_void_p),
+                                            len(arrs), M, ch.ctypes.data if len(ch) else None, len(ch), _ptr(W),
+                                            _stream_ptr(arrs[0], stream)))
+    return _mat_out(W)
+
+
+def whiten_clips(clips, W, quantization_unit=0.0, out=None, stream=None, precision="plain"):
+    """ms3.whiten_clips (p_whiten.cpp:300-345): clips as an (L, T, M) array
+    (the .mda M x T x L layout); W^T x at every timepoint, no 1e-4 rounding;
+    int16 when quantization_unit > 0."""
+    L_ = _lib.load()
+    c = _as_f32_rows(clips)
+    if c.ndim != 3:
+        raise ValueError("clips must be (L, T, M)")
+    L, T, M = c.shape
+    Wc = _mat_in(W, c)
+    if out is None:
+        out = _empty_like(c, (L, T, M), np.int16 if quantization_unit > 0 else np.float32)
+    check(L_.ms3gpu_whiten_clips(_ptr(c), M, T, L, _ptr(Wc), float(quantization_unit), _PRECISION[precision],
+                                 _ptr(out), _stream_ptr(c, stream)))
+    return out
+
+
 def requirements(processor: str, M: int, N: int, **params) -> float:
     """The processor's peak-RAM model in MB (its "requirements" answer)."""
     L = _lib.load()

@@ -128,13 +128,14 @@ __device__ __forceinline__ void store_row32(const float (&y)[32], int64_t t, int
     }
 }
 
-// Rounds 32 values of one timepoint to 1e-4 and writes them: float output
+// Rounds 32 values of one timepoint to 1e-4 (unless round_1e4 is 0) and writes them: float output
 // through the warp's swizzled staging buffer and one TMA store of the warp's
 // 32 x 32 block (full 128-byte lines), int16 output directly.
 __device__ __forceinline__ void emit_row32(float (&y)[32], int lane, uint8_t* staging_warp, int& sbuf,
                                            const CUtensorMap* tmOut, int out_tma, int64_t t, int64_t trow0, int n,
-                                           int64_t M, int64_t N, double qunit, void* __restrict__ out) {
-    quantize_1e4_x32(y);
+                                           int64_t M, int64_t N, double qunit, int round_1e4,
+                                           void* __restrict__ out) {
+    if (round_1e4) quantize_1e4_x32(y);
     if (out_tma) {
         uint8_t* stg = staging_warp + (size_t)sbuf * (32 * 128);
         if (lane == 0) tc::bulk_wait_group_read<1>();  // its previous store has read it
@@ -176,8 +177,8 @@ template <int BN, bool DRAIN>
 __global__ void __launch_bounds__(TcCfg<BN, DRAIN>::kThreads, 1)
     apply_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmWhi,
                     const __grid_constant__ CUtensorMap tmWlo, const __grid_constant__ CUtensorMap tmOut, int out_tma,
-                    int64_t M, int64_t N, int ncb, int64_t ntiles, double qunit, void* __restrict__ out,
-                    int* __restrict__ err) {
+                    int64_t M, int64_t N, int ncb, int64_t ntiles, double qunit, int round_1e4,
+                    void* __restrict__ out, int* __restrict__ err) {
     using C = TcCfg<BN, DRAIN>;
     constexpr int S = C::kStages;
     constexpr int R = 2;  // accumulator ring (K-blocks when DRAIN, tiles when mixed)
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(TcCfg<BN, DRAIN>::kThreads, 1)
                     float y[32];
 #pragma unroll
                     for (int j = 0; j < 32; j++) y[j] = __uint_as_float(r[j]);
-                    emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, out);
+                    emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, round_1e4, out);
                 }
                 tc::tc_fence_before();
                 tc::mbar_arrive(&acc_free[tp]);
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(TcCfg<BN, DRAIN>::kThreads, 1)
                 float y[32];
 #pragma unroll
                 for (int j = 0; j < 32; j++) y[j] = __uint_as_float(r[j]);
-                emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, out);
+                emit_row32(y, lane, stg, sbuf, &tmOut, out_tma, t, t0 + q * 32, n0 + c0, M, N, qunit, round_1e4, out);
             }
         }
         if (out_tma && lane == 0) tc::bulk_wait_group<0>();  // stores complete before the CTA exits
@@ -472,7 +473,7 @@ CUtensorMap make_map(const void* base, uint64_t cols, uint64_t rows, uint32_t bo
 
 template <int BN, bool DRAIN>
 void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, const float* wlo, double qunit,
-                     void* out, int* err, cudaStream_t stream) {
+                     int round_1e4, void* out, int* err, cudaStream_t stream) {
     using C = TcCfg<BN, DRAIN>;
     MS3_CUDA(cudaFuncSetAttribute(apply_tc_kernel<BN, DRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)C::kSmemBytes));
@@ -489,7 +490,8 @@ void launch_apply_tc(const float* X, int64_t M, int64_t N, const float* whi, con
     MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(ntiles, nsm);  // one persistent CTA per SM
     apply_tc_kernel<BN, DRAIN><<<(unsigned)grid, C::kThreads, C::kSmemBytes, stream>>>(mx, mh, ml, mo, out_tma, M, N, ncb,
-                                                                                     ntiles, qunit, out, err);
+                                                                                     ntiles, qunit, round_1e4,
+                                                                                     out, err);
     MS3_LAUNCH_CHECK();
 }
 
@@ -503,7 +505,7 @@ bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out) {
 }
 
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        bool drain, void* out, cudaStream_t stream, int* ext_err) {
+                        bool drain, void* out, cudaStream_t stream, int* ext_err, bool round_1e4) {
     DevBuf wbuf(sizeof(float) * (size_t)(2 * M * M) + 256, stream);
     float* whi = wbuf.as<float>();
     float* wlo = whi + M * M;
@@ -512,9 +514,9 @@ void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, d
     w_split_tf32<<<(unsigned)ceil_div(M * M, 256), 256, 0, stream>>>(W, M * M, whi, wlo);
     MS3_LAUNCH_CHECK();
     if (drain)
-        launch_apply_tc<128, true>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+        launch_apply_tc<128, true>(X, M, N, whi, wlo, quantization_unit, round_1e4 ? 1 : 0, out, err, stream);
     else
-        launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, out, err, stream);
+        launch_apply_tc<128, false>(X, M, N, whi, wlo, quantization_unit, round_1e4 ? 1 : 0, out, err, stream);
     if (ext_err) return;  // the caller checks the flag once for many calls
     int herr = 0;
     MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));

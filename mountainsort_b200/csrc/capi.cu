@@ -14,6 +14,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "bandpass.h"
 #include "common.cuh"
@@ -353,6 +354,97 @@ int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N,
         out.setup(timeseries_out, out_bytes, s);
         apply_whitening_device(static_cast<const float*>(in.ptr), M, N, static_cast<const double*>(w.ptr),
                                quantization_unit, check_precision(precision), out.ptr, s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const int64_t* N_list, int32_t n_inputs,
+                                    int64_t M, const int32_t* channels, int32_t n_channels, double* W_out,
+                                    void* stream) {
+    return guarded([&] {
+        if (n_inputs < 1) throw_invalid("timeseries_list is empty");
+        require(timeseries_list, "timeseries_list", true);
+        require(N_list, "N_list", true);
+        if (M <= 0) throw_invalid("M must be positive");
+        if (n_channels < 0) throw_invalid("n_channels is negative");
+        require(channels, "channels", n_channels > 0);
+        require(W_out, "W_out", true);
+        const int64_t M2 = n_channels > 0 ? n_channels : M;
+        std::vector<int32_t> ch0((size_t)M2);
+        for (int64_t j = 0; j < M2; j++) {
+            const int64_t c = n_channels > 0 ? channels[j] : j + 1;
+            if (c < 1 || c > M)
+                throw_invalid("channel " + std::to_string(c) + " is outside 1.." + std::to_string(M));
+            ch0[(size_t)j] = (int32_t)(c - 1);
+        }
+        int64_t Ntot = 0;
+        for (int32_t i = 0; i < n_inputs; i++) {
+            check_shape(M, N_list[i]);
+            require(timeseries_list[i], "timeseries_list entry", N_list[i] > 0);
+            Ntot += N_list[i];
+        }
+        cudaStream_t s = as_stream(stream);
+        DevBuf chmap;
+        if (n_channels > 0) {
+            chmap.alloc(sizeof(int32_t) * (size_t)M2, s);
+            MS3_CUDA(cudaMemcpyAsync(chmap.get(), ch0.data(), sizeof(int32_t) * (size_t)M2, cudaMemcpyHostToDevice, s));
+        }
+        // the recordings' partial tiles go to consecutive slices of one buffer
+        const CovPlan plan = cov_plan(nullptr, M2);
+        std::vector<int64_t> slices((size_t)n_inputs);
+        int64_t Stot = 0;
+        for (int32_t i = 0; i < n_inputs; i++) Stot += (slices[(size_t)i] = cov_slices(plan, N_list[i]));
+        DevBuf partials(cov_partials_bytes(plan, Stot), s);
+        int64_t done = 0;
+        for (int32_t i = 0; i < n_inputs; i++) {
+            const int64_t Ni = N_list[i];
+            if (Ni == 0) continue;
+            InView in;
+            stage_in(in, timeseries_list[i], sizeof(float) * (size_t)(M * Ni), s);
+            const float* X = static_cast<const float*>(in.ptr);
+            DevBuf sub;
+            if (n_channels > 0) {
+                sub.alloc(sizeof(float) * (size_t)(M2 * Ni), s);
+                gather_channels_device(X, M, Ni, chmap.as<int32_t>(), M2, sub.as<float>(), s);
+                X = sub.as<float>();
+            }
+            double* part_i = reinterpret_cast<double*>(partials.as<char>() + cov_partials_bytes(plan, done));
+            cov_partials(X, M2, 0, Ni, cov_plan(X, M2), part_i, slices[(size_t)i], s);
+            done += slices[(size_t)i];
+        }
+        DevBuf xxt(sizeof(double) * (size_t)(M2 * M2), s);
+        cov_finish(partials.as<double>(), Stot, plan, M2, Ntot, xxt.as<double>(), s);
+        OutView w;
+        w.setup(W_out, sizeof(double) * (size_t)(M2 * M2), s);
+        whitening_matrix_device(xxt.as<double>(), M2, static_cast<double*>(w.ptr), nullptr, nullptr, s);
+        w.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* W,
+                        double quantization_unit, int32_t precision, void* clips_out, void* stream) {
+    return guarded([&] {
+        if (T < 0 || L < 0) throw_invalid("negative dimension");
+        if (T > 0 && L > std::numeric_limits<int64_t>::max() / T) throw_invalid("clips too large");
+        const int64_t N = T * L;
+        check_shape(M, N);
+        cudaStream_t s = as_stream(stream);
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        const size_t out_bytes = (quantization_unit > 0 ? 2 : 4) * (size_t)(M * N);
+        require(clips, "clips", in_bytes > 0);
+        require(clips_out, "clips_out", out_bytes > 0);
+        require(W, "W", M > 0);
+        InView in, w;
+        stage_in(in, clips, in_bytes, s);
+        stage_in(w, W, sizeof(double) * (size_t)(M * M), s);
+        OutView out;
+        out.setup(clips_out, out_bytes, s);
+        // the clips' timepoints, clip after clip, are one M x (T*L) array
+        apply_whitening_device(static_cast<const float*>(in.ptr), M, N, static_cast<const double*>(w.ptr),
+                               quantization_unit, check_precision(precision), out.ptr, s, nullptr,
+                               /*round_1e4=*/false);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
     });

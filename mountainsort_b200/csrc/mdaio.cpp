@@ -17,9 +17,9 @@ struct FileCloser {
 };
 using FilePtr = std::unique_ptr<FILE, FileCloser>;
 
-template <class S>
-void convert(const S* src, float* dst, int64_t n) {
-    for (int64_t i = 0; i < n; i++) dst[i] = (float)src[i];
+template <class S, class D>
+void convert(const S* src, D* dst, int64_t n) {
+    for (int64_t i = 0; i < n; i++) dst[i] = (D)src[i];
 }
 }  // namespace
 
@@ -155,6 +155,95 @@ bool copy_file(const std::string& src, const std::string& dst, std::string& err)
     size_t n;
     while ((n = std::fread(buf.data(), 1, buf.size(), in.get())) > 0)
         if (std::fwrite(buf.data(), 1, n, out.get()) != n) { err = "write failed for " + dst; return false; }
+    return true;
+}
+
+}  // namespace ms3io
+
+namespace ms3io {
+
+namespace {
+// All entries of an array converted to D (std::copy semantics, like the
+// reference's mdaReadData, mdaio.cpp:205-230).
+template <class D>
+bool read_entries(const std::string& path, std::vector<int64_t>& dims, std::vector<D>& data, std::string& err) {
+    MdaHeader h;
+    if (!read_header(path, h, err)) return false;
+    FilePtr f(std::fopen(path.c_str(), "rb"));
+    if (!f) { err = "cannot open " + path; return false; }
+    std::fseek(f.get(), (long)h.header_size, SEEK_SET);
+    dims = h.dims;
+    int64_t n = 1;
+    for (int64_t d : dims) n *= d;
+    data.resize((size_t)n);
+    const int64_t block = 1 << 20;
+    const int bpe = h.bytes_per_entry;
+    std::vector<unsigned char> buf((size_t)(block * bpe));
+    for (int64_t i = 0; i < n; i += block) {
+        const int64_t m = std::min(block, n - i);
+        if ((int64_t)std::fread(buf.data(), (size_t)bpe, (size_t)m, f.get()) != m) { err = "short read from " + path; return false; }
+        D* dst = data.data() + i;
+        switch (h.data_type) {
+            case kUint8: convert(reinterpret_cast<const uint8_t*>(buf.data()), dst, m); break;
+            case kFloat32: convert(reinterpret_cast<const float*>(buf.data()), dst, m); break;
+            case kInt16: convert(reinterpret_cast<const int16_t*>(buf.data()), dst, m); break;
+            case kInt32: convert(reinterpret_cast<const int32_t*>(buf.data()), dst, m); break;
+            case kUint16: convert(reinterpret_cast<const uint16_t*>(buf.data()), dst, m); break;
+            case kFloat64: convert(reinterpret_cast<const double*>(buf.data()), dst, m); break;
+            case kUint32: convert(reinterpret_cast<const uint32_t*>(buf.data()), dst, m); break;
+            default: err = "unsupported data type"; return false;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+bool read_array_f32(const std::string& path, std::vector<int64_t>& dims, std::vector<float>& data,
+                    std::string& err) {
+    return read_entries(path, dims, data, err);
+}
+
+bool read_array_f64(const std::string& path, std::vector<int64_t>& dims, std::vector<double>& data,
+                    std::string& err) {
+    return read_entries(path, dims, data, err);
+}
+
+bool write_array(const std::string& path, int32_t data_type, const std::vector<int64_t>& dims, const void* data,
+                 std::string& err) {
+    const std::string tmp = path + ".tmp";
+    std::remove(path.c_str());
+    FilePtr f(std::fopen(tmp.c_str(), "wb"));
+    if (!f) { err = "cannot open " + tmp + " for writing"; return false; }
+    bool use64 = false;
+    int64_t n = 1;
+    for (int64_t d : dims) {
+        use64 = use64 || d > 2e9;
+        n *= d;
+    }
+    const int32_t nd = (int32_t)dims.size();
+    const int32_t hdr[3] = {data_type, (int32_t)bytes_per_entry(data_type), use64 ? -nd : nd};
+    bool ok = std::fwrite(hdr, 4, 3, f.get()) == 3;
+    for (int64_t d : dims) {
+        if (use64) {
+            ok = ok && std::fwrite(&d, 8, 1, f.get()) == 1;
+        } else {
+            const int32_t d32 = (int32_t)d;
+            ok = ok && std::fwrite(&d32, 4, 1, f.get()) == 1;
+        }
+    }
+    if (n) ok = ok && std::fwrite(data, (size_t)bytes_per_entry(data_type), (size_t)n, f.get()) == (size_t)n;
+    ok = ok && std::fflush(f.get()) == 0;
+    FILE* raw = f.release();
+    ok = (std::fclose(raw) == 0) && ok;
+    if (!ok) {
+        std::remove(tmp.c_str());
+        err = "write failed for " + tmp;
+        return false;
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+        err = "cannot rename " + tmp + " to " + path;
+        return false;
+    }
     return true;
 }
 

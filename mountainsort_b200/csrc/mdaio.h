@@ -37,6 +37,16 @@ bool read_timeseries_f32(const std::string& path, int64_t& M, int64_t& N, std::v
 bool write_timeseries(const std::string& path, int32_t data_type, int64_t M, int64_t N, const void* data,
                       std::string& err);
 
+// Every entry of an N-dimensional array, converted to float32 / float64.
+bool read_array_f32(const std::string& path, std::vector<int64_t>& dims, std::vector<float>& data,
+                    std::string& err);
+bool read_array_f64(const std::string& path, std::vector<int64_t>& dims, std::vector<double>& data,
+                    std::string& err);
+
+// Writes an N-dimensional array of `data_type` (via path.tmp + rename).
+bool write_array(const std::string& path, int32_t data_type, const std::vector<int64_t>& dims, const void* data,
+                 std::string& err);
+
 // Byte copy that, like QFile::copy, refuses to overwrite an existing file.
 bool copy_file(const std::string& src, const std::string& dst, std::string& err);
 

@@ -1,5 +1,6 @@
-// ms3gpu.mp -- MountainLab processor executable for ms3.bandpass_filter and
-// ms3.whiten, backed by libms3gpu (CUDA, sm_100a).
+// ms3gpu.mp -- MountainLab processor executable for ms3.bandpass_filter,
+// ms3.whiten, ms3.compute_whitening_matrix, ms3.apply_whitening_matrix and
+// ms3.whiten_clips, backed by libms3gpu (CUDA, sm_100a).
 //
 // Same command-line protocol as the reference's ms3.mp
 // (packages/ms3/mountainsort3_main.cpp:379-821):
@@ -26,9 +27,12 @@
 namespace {
 
 // CLParams (packages/ms3/common/clparams.cpp:20-77): "--name=value" or
-// "--name value"; everything else is an unnamed parameter.
+// "--name value"; everything else is an unnamed parameter.  A name given
+// more than once becomes a list (:55-68): `lists` keeps every value in
+// order, `named` the last one.
 struct CLParams {
     std::map<std::string, std::string> named;
+    std::map<std::string, std::vector<std::string>> lists;
     std::vector<std::string> unnamed;
     bool success = true;
     std::string error;
@@ -51,6 +55,7 @@ struct CLParams {
                     return;
                 }
                 named[name] = val;
+                lists[name].push_back(val);
             } else {
                 unnamed.push_back(s);
             }
@@ -98,7 +103,8 @@ struct Param {
 // QJsonObject serialises them.
 std::string processor_spec(const std::string& name, const std::string& version,
                            const std::vector<std::string>& inputs, const std::vector<std::string>& outputs,
-                           const std::vector<Param>& params, const std::string& ind) {
+                           const std::vector<Param>& params, const std::string& ind,
+                           bool can_return_requirements = true) {
     const std::string exe = exe_path();
     auto files = [&](const std::vector<std::string>& v) {
         std::string o = "[\n";
@@ -126,7 +132,8 @@ std::string processor_spec(const std::string& name, const std::string& version,
     o += ind + "    \"name\": \"" + name + "\",\n";
     o += ind + "    \"outputs\": " + files(outputs) + ",\n";
     o += ind + "    \"parameters\": " + ps + ",\n";
-    o += ind + "    \"requirements_command\": \"" + json_escape(exe) + " requirements " + name + " $(arguments)\",\n";
+    if (can_return_requirements)
+        o += ind + "    \"requirements_command\": \"" + json_escape(exe) + " requirements " + name + " $(arguments)\",\n";
     o += ind + "    \"version\": \"" + version + "\"\n";
     o += ind + "}";
     return o;
@@ -147,6 +154,19 @@ std::string spec_bandpass(const std::string& ind) {
 std::string spec_whiten(const std::string& ind) {
     return processor_spec("ms3.whiten", "0.1", {"timeseries"}, {"timeseries_out"},
                           {{"quantization_unit", true, "0"}}, ind);
+}
+// mountainsort3_main.cpp:166-189 (no requirements command for these)
+std::string spec_compute_whitening_matrix(const std::string& ind) {
+    return processor_spec("ms3.compute_whitening_matrix", "0.11", {"timeseries_list"}, {"whitening_matrix_out"},
+                          {{"channels", true, ""}}, ind, false);
+}
+std::string spec_whiten_clips(const std::string& ind) {
+    return processor_spec("ms3.whiten_clips", "0.1", {"clips", "whitening_matrix"}, {"clips_out"},
+                          {{"quantization_unit", true, "0"}}, ind, false);
+}
+std::string spec_apply_whitening_matrix(const std::string& ind) {
+    return processor_spec("ms3.apply_whitening_matrix", "0.1", {"timeseries", "whitening_matrix"},
+                          {"timeseries_out"}, {{"quantization_unit", true, "0"}}, ind, false);
 }
 
 // T of the chunk-size formula: omp_get_max_threads() in the reference, set
@@ -183,6 +203,11 @@ void print_requirements(double mb) { std::printf("{\n    \"peak_ram_mb\": %.17g\
 int fail(const std::string& msg) {
     std::fprintf(stderr, "ms3gpu: %s\n", msg.c_str());
     return -1;
+}
+
+int32_t precision_of(const CLParams& clp) {
+    // --_precision=mixed selects the mixed form (not a reference parameter)
+    return clp.str("_precision") == "mixed" ? MS3GPU_PRECISION_MIXED : MS3GPU_PRECISION_PLAIN;
 }
 
 int run_bandpass(const CLParams& clp, bool requirements_only) {
@@ -226,8 +251,7 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
     const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
     ms3gpu_whiten_opts o;
     o.quantization_unit = clp.num("quantization_unit", 0);  // mountainsort3_main.cpp:576
-    // --_precision=mixed selects the tensor-core apply (not a reference parameter)
-    o.precision = clp.str("_precision") == "mixed" ? MS3GPU_PRECISION_MIXED : MS3GPU_PRECISION_PLAIN;
+    o.precision = precision_of(clp);
     std::string err;
     ms3io::MdaHeader h;
     if (!ms3io::read_header(in, h, err)) return fail(err);
@@ -252,6 +276,98 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
     return 0;
 }
 
+// A whitening matrix file (Mda WW(path): any dtype, read as double), M x M.
+bool read_whitening_matrix(const std::string& path, int64_t M, std::vector<double>& W, std::string& err) {
+    std::vector<int64_t> dims;
+    if (!ms3io::read_array_f64(path, dims, W, err)) return false;
+    const int64_t n1 = dims.size() > 0 ? dims[0] : 1, n2 = dims.size() > 1 ? dims[1] : 1;
+    if (n1 != M || n2 != M || (int64_t)W.size() != M * M) {
+        err = "whitening matrix " + path + " is not " + std::to_string(M) + " x " + std::to_string(M);
+        return false;
+    }
+    return true;
+}
+
+// p_compute_whitening_matrix (p_whiten.cpp:208-298) with the arguments of
+// mountainsort3_main.cpp:594-600.
+int run_compute_whitening_matrix(const CLParams& clp) {
+    auto it = clp.lists.find("timeseries_list");
+    if (it == clp.lists.end() || it->second.empty()) return fail("timeseries_list is empty");
+    const std::string out = clp.str("whitening_matrix_out");
+    std::vector<int32_t> channels;
+    {
+        // split(",", SkipEmptyParts) then toInt (0 for a non-number)
+        const std::string cs = clp.str("channels");
+        size_t a = 0;
+        while (a <= cs.size()) {
+            size_t b = cs.find(',', a);
+            if (b == std::string::npos) b = cs.size();
+            if (b > a) channels.push_back((int32_t)std::atoi(cs.substr(a, b - a).c_str()));
+            a = b + 1;
+        }
+    }
+    std::vector<std::vector<float>> data(it->second.size());
+    std::vector<const float*> ptrs;
+    std::vector<int64_t> Ns;
+    int64_t M = -1;
+    std::string err;
+    for (size_t i = 0; i < it->second.size(); i++) {
+        int64_t Mi = 0, Ni = 0;
+        if (!ms3io::read_timeseries_f32(it->second[i], Mi, Ni, data[i], err)) return fail(err);
+        if (M >= 0 && Mi != M) return fail("the recordings of timeseries_list differ in channel count");
+        M = Mi;
+        ptrs.push_back(data[i].data());
+        Ns.push_back(Ni);
+    }
+    const int64_t M2 = channels.empty() ? M : (int64_t)channels.size();
+    std::vector<double> W((size_t)(M2 * M2));
+    if (ms3gpu_compute_whitening_matrix(ptrs.data(), Ns.data(), (int32_t)ptrs.size(), M,
+                                        channels.empty() ? nullptr : channels.data(), (int32_t)channels.size(),
+                                        W.data(), nullptr) != MS3GPU_OK)
+        return fail(ms3gpu_last_error());
+    // Mda::write64 (float64)
+    if (!ms3io::write_array(out, ms3io::kFloat64, {M2, M2}, W.data(), err)) return fail(err);
+    return 0;
+}
+
+// p_apply_whitening_matrix (p_whiten.cpp:347-417)
+int run_apply_whitening_matrix(const CLParams& clp) {
+    const std::string in = clp.str("timeseries"), wpath = clp.str("whitening_matrix"), out = clp.str("timeseries_out");
+    const double q = clp.num("quantization_unit", 0);
+    std::string err;
+    std::vector<float> X;
+    int64_t M = 0, N = 0;
+    if (!ms3io::read_timeseries_f32(in, M, N, X, err)) return fail(err);
+    std::vector<double> W;
+    if (!read_whitening_matrix(wpath, M, W, err)) return fail(err);
+    const bool i16 = q > 0;
+    std::vector<unsigned char> Y((size_t)(M * N) * (i16 ? 2 : 4));
+    if (ms3gpu_apply_whitening_matrix(X.data(), M, N, W.data(), q, precision_of(clp), Y.data(), nullptr) != MS3GPU_OK)
+        return fail(ms3gpu_last_error());
+    if (!ms3io::write_timeseries(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    return 0;
+}
+
+// p_whiten_clips (p_whiten.cpp:300-345): clips M x T x L
+int run_whiten_clips(const CLParams& clp) {
+    const std::string in = clp.str("clips"), wpath = clp.str("whitening_matrix"), out = clp.str("clips_out");
+    const double q = clp.num("quantization_unit", 0);
+    std::string err;
+    std::vector<int64_t> dims;
+    std::vector<float> C;
+    if (!ms3io::read_array_f32(in, dims, C, err)) return fail(err);
+    const int64_t M = dims.size() > 0 ? dims[0] : 1, T = dims.size() > 1 ? dims[1] : 1;
+    const int64_t L = (M * T) ? (int64_t)C.size() / (M * T) : 0;
+    std::vector<double> W;
+    if (!read_whitening_matrix(wpath, M, W, err)) return fail(err);
+    const bool i16 = q > 0;
+    std::vector<unsigned char> Y((size_t)(M * T * L) * (i16 ? 2 : 4));
+    if (ms3gpu_whiten_clips(C.data(), M, T, L, W.data(), q, precision_of(clp), Y.data(), nullptr) != MS3GPU_OK)
+        return fail(ms3gpu_last_error());
+    if (!ms3io::write_array(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, {M, T, L}, Y.data(), err)) return fail(err);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -260,18 +376,22 @@ int main(int argc, char** argv) {
     const std::string arg1 = clp.unnamed.size() > 0 ? clp.unnamed[0] : "";
     const std::string arg2 = clp.unnamed.size() > 1 ? clp.unnamed[1] : "";
     if (arg1 == "spec") {
+        std::string (*const specs[])(const std::string&) = {spec_bandpass, spec_whiten,
+                                                             spec_compute_whitening_matrix, spec_whiten_clips,
+                                                             spec_apply_whitening_matrix};
+        const char* const names[] = {"ms3.bandpass_filter", "ms3.whiten", "ms3.compute_whitening_matrix",
+                                     "ms3.whiten_clips", "ms3.apply_whitening_matrix"};
         if (arg2.empty()) {
-            std::printf("{\n    \"processors\": [\n%s,\n%s\n    ]\n}\n\n", spec_bandpass("        ").c_str(),
-                        spec_whiten("        ").c_str());
+            std::string all;
+            for (size_t i = 0; i < 5; i++) all += (i ? ",\n" : "") + specs[i]("        ");
+            std::printf("{\n    \"processors\": [\n%s\n    ]\n}\n\n", all.c_str());
             return 0;
         }
-        if (arg2 == "ms3.bandpass_filter") {
-            std::printf("%s\n\n", spec_bandpass("").c_str());
-            return 0;
-        }
-        if (arg2 == "ms3.whiten") {
-            std::printf("%s\n\n", spec_whiten("").c_str());
-            return 0;
+        for (size_t i = 0; i < 5; i++) {
+            if (arg2 == names[i]) {
+                std::printf("%s\n\n", specs[i]("").c_str());
+                return 0;
+            }
         }
         std::printf("{}\n");
         return -1;
@@ -284,6 +404,11 @@ int main(int argc, char** argv) {
     }
     if (pname == "ms3.bandpass_filter") return run_bandpass(clp, requirements_only);
     if (pname == "ms3.whiten") return run_whiten(clp, requirements_only);
+    if (!requirements_only) {
+        if (pname == "ms3.compute_whitening_matrix") return run_compute_whitening_matrix(clp);
+        if (pname == "ms3.apply_whitening_matrix") return run_apply_whitening_matrix(clp);
+        if (pname == "ms3.whiten_clips") return run_whiten_clips(clp);
+    }
     std::fprintf(stderr, "Unexpected processor name: %s\n", pname.c_str());
     return -1;
 }

@@ -410,7 +410,8 @@ __device__ __forceinline__ float quantize_1e4(float x) {
 constexpr int kBM = 64, kBN = 64, kBK = 16;
 
 __global__ void __launch_bounds__(256) apply_gemm(const float* __restrict__ X, const float* __restrict__ Wt,
-                                                  int64_t M, int64_t N, double qunit, void* __restrict__ out) {
+                                                  int64_t M, int64_t N, double qunit, int round_1e4,
+                                                  void* __restrict__ out) {
     __shared__ __align__(16) float Xs[kBK][kBM + 4];
     __shared__ __align__(16) float Ws[kBK][kBN + 4];
     // column blocks of one time tile are adjacent in launch order, so the
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(256) apply_gemm(const float* __restrict__ X, c
         for (int j = 0; j < 4; j++) {
             const int64_t n = n0 + tx * 4 + j;
             if (n >= M) continue;
-            const float y = quantize_1e4(acc[i][j]);
+            const float y = round_1e4 ? quantize_1e4(acc[i][j]) : acc[i][j];
             if (qunit > 0) {
                 // scale_for_quantization (p_whiten.cpp:445-451): (int)(y/q + 0.5)
                 // stored in a float, then written as int16 by the .mda writer.
@@ -464,6 +465,18 @@ __global__ void __launch_bounds__(256) apply_gemm(const float* __restrict__ X, c
                 static_cast<float*>(out)[t * M + n] = y;
             }
         }
+    }
+}
+
+// out[t][j] = X[t][ch[j]] for a channel subset (0-based indices, checked by
+// the caller): ms3.compute_whitening_matrix's extract_channels_from_chunk
+// (p_whiten.cpp:421-433) applied to a whole device array.
+__global__ void gather_channels(const float* __restrict__ X, int64_t M, int64_t N, const int32_t* __restrict__ ch,
+                                int64_t M2, float* __restrict__ out) {
+    const int64_t total = N * M2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = i / M2, j = i - t * M2;
+        out[i] = X[t * M + ch[j]];
     }
 }
 
@@ -647,14 +660,22 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
     MS3_LAUNCH_CHECK();
 }
 
+void gather_channels_device(const float* X, int64_t M, int64_t N, const int32_t* ch, int64_t M2, float* out,
+                            cudaStream_t stream) {
+    if (N <= 0 || M2 <= 0) return;
+    const int64_t blocks = std::min<int64_t>(ceil_div(N * M2, 256), (int64_t)num_sms() * 32);
+    gather_channels<<<(unsigned)blocks, 256, 0, stream>>>(X, M, N, ch, M2, out);
+    MS3_LAUNCH_CHECK();
+}
+
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                            bool mixed, void* out, cudaStream_t stream, int* err) {
+                            bool mixed, void* out, cudaStream_t stream, int* err, bool round_1e4) {
     if (M <= 0 || N <= 0) return;
     // MS3GPU_APPLY_FFMA=1 selects the FP32 FMA kernel for the plain form
     const char* ffma = std::getenv("MS3GPU_APPLY_FFMA");
     const bool force_ffma = ffma && ffma[0] == '1';
     if (apply_tc_supported(X, M, N, out) && (mixed || !force_ffma)) {
-        apply_whitening_tc(X, M, N, W, quantization_unit, /*drain=*/!mixed, out, stream, err);
+        apply_whitening_tc(X, M, N, W, quantization_unit, /*drain=*/!mixed, out, stream, err, round_1e4);
         return;
     }
     DevBuf wt(sizeof(float) * (size_t)(M * M), stream);
@@ -662,7 +683,8 @@ void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* 
     MS3_LAUNCH_CHECK();
     const int64_t blocks = ceil_div(N, kBM) * ceil_div(M, kBN);
     if (blocks > 0x7fffffff) throw_unsupported("too many tiles for the apply kernel");
-    apply_gemm<<<(unsigned)blocks, 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, out);
+    apply_gemm<<<(unsigned)blocks, 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, round_1e4 ? 1 : 0,
+                                                     out);
     MS3_LAUNCH_CHECK();
 }
 

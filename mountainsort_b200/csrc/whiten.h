@@ -30,6 +30,10 @@ void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, 
 void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
 int64_t covariance_noalloc_max_channels();
 
+// out (N x M2 rows) = the channels ch[0..M2) (0-based, in range) of X (N x M rows).
+void gather_channels_device(const float* X, int64_t M, int64_t N, const int32_t* ch, int64_t M2, float* out,
+                            cudaStream_t stream);
+
 // Power-iteration whitening matrix; comps / sigma may be null.
 void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
                              cudaStream_t stream);
@@ -39,9 +43,11 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
 // allow), else FP32 FMA.
 // err: optional device flag raised by a timed-out tensor-core pipeline; when
 // null the call checks it itself (synchronising the stream).
+// round_1e4 = false skips the 1e-4 rounding (ms3.whiten_clips, which does
+// not round, p_whiten.cpp:300-345).
 void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* W,
                             double quantization_unit, bool mixed, void* out, cudaStream_t stream,
-                            int* err = nullptr);
+                            int* err = nullptr, bool round_1e4 = true);
 
 // Tensor-core (tcgen05, 3-term TF32) apply; apply_tc_supported tells whether
 // the shapes and alignment allow it.
@@ -49,6 +55,6 @@ bool apply_tc_supported(const float* X, int64_t M, int64_t N, const void* out);
 // drain: per-K-block draining of the large products into round-to-nearest
 // FP32 sums (plain form); otherwise one FP32 TMEM accumulator (mixed form).
 void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, double quantization_unit,
-                        bool drain, void* out, cudaStream_t stream, int* err = nullptr);
+                        bool drain, void* out, cudaStream_t stream, int* err = nullptr, bool round_1e4 = true);
 
 }  // namespace ms3gpu

@@ -1,7 +1,8 @@
-"""File-level mirror of the reference's two processors, for Python callers.
+"""File-level mirror of the reference's whitening and filter processors, for
+Python callers.
 
 The same names, parameters, defaults and output dtypes as the reference's
-ms3.mp (packages/ms3/mountainsort3_main.cpp:146-165, 547-591): each function
+ms3.mp (packages/ms3/mountainsort3_main.cpp:146-189, 547-615): each function
 reads the input .mda, runs the GPU path and writes the output .mda (via
 path.tmp and a rename).  Returns True on success like the reference's
 processor functions; errors raise Ms3GpuError / MdaError.  The C++
@@ -27,6 +28,24 @@ SPEC = {
     "ms3.whiten": {
         "version": "0.1",
         "inputs": ["timeseries"],
+        "outputs": ["timeseries_out"],
+        "parameters": [("quantization_unit", True, 0)],
+    },
+    "ms3.compute_whitening_matrix": {
+        "version": "0.11",
+        "inputs": ["timeseries_list"],
+        "outputs": ["whitening_matrix_out"],
+        "parameters": [("channels", True, None)],
+    },
+    "ms3.whiten_clips": {
+        "version": "0.1",
+        "inputs": ["clips", "whitening_matrix"],
+        "outputs": ["clips_out"],
+        "parameters": [("quantization_unit", True, 0)],
+    },
+    "ms3.apply_whitening_matrix": {
+        "version": "0.1",
+        "inputs": ["timeseries", "whitening_matrix"],
         "outputs": ["timeseries_out"],
         "parameters": [("quantization_unit", True, 0)],
     },
@@ -64,7 +83,64 @@ def whiten(timeseries, timeseries_out, quantization_unit=0) -> bool:
     return True
 
 
-PROCESSORS = {"ms3.bandpass_filter": bandpass_filter, "ms3.whiten": whiten}
+def _parse_channels(channels):
+    # split(",", SkipEmptyParts) + toInt, mountainsort3_main.cpp:597-598
+    if channels is None or channels == "":
+        return None
+    if isinstance(channels, str):
+        out = []
+        for part in channels.split(","):
+            if part:
+                try:
+                    out.append(int(part))
+                except ValueError:
+                    out.append(0)
+        return out or None
+    return [int(c) for c in channels]
+
+
+def _read_matrix(path, M):
+    W = np.asarray(mdaio.readmda(path), dtype=np.float64)
+    if W.shape[:2] != (M, M):
+        raise ValueError(f"whitening matrix {path} is not {M} x {M}")
+    return W
+
+
+def compute_whitening_matrix(timeseries_list, whitening_matrix_out, channels=None) -> bool:
+    """ms3.compute_whitening_matrix (p_whiten.cpp:208-298); writes float64."""
+    if isinstance(timeseries_list, str):
+        timeseries_list = [timeseries_list]
+    Xs = [_read_rows(p) for p in timeseries_list]
+    W = api.compute_whitening_matrix(Xs, channels=_parse_channels(channels))
+    mdaio.writemda(np.asarray(W, dtype=np.float64), whitening_matrix_out, dtype="float64")
+    return True
+
+
+def apply_whitening_matrix(timeseries, whitening_matrix, timeseries_out, quantization_unit=0) -> bool:
+    """ms3.apply_whitening_matrix (p_whiten.cpp:347-417)."""
+    X = _read_rows(timeseries)
+    W = _read_matrix(whitening_matrix, X.shape[1])
+    Y = api.apply_whitening_matrix(X, W, quantization_unit=float(quantization_unit))
+    mdaio.writemda(Y.T, timeseries_out)
+    return True
+
+
+def whiten_clips(clips, whitening_matrix, clips_out, quantization_unit=0) -> bool:
+    """ms3.whiten_clips (p_whiten.cpp:300-345): clips M x T x L."""
+    C = np.asarray(mdaio.readmda(clips), dtype=np.float32)
+    while C.ndim < 3:
+        C = C[..., None]
+    M, T, L = C.shape[0], C.shape[1], int(np.prod(C.shape[2:]))
+    rows = np.ascontiguousarray(C.reshape(M, T, L, order="F").transpose(2, 1, 0))  # (L, T, M)
+    W = _read_matrix(whitening_matrix, M)
+    Y = api.whiten_clips(rows, W, quantization_unit=float(quantization_unit))
+    mdaio.writemda(np.asarray(Y).transpose(2, 1, 0), clips_out)
+    return True
+
+
+PROCESSORS = {"ms3.bandpass_filter": bandpass_filter, "ms3.whiten": whiten,
+              "ms3.compute_whitening_matrix": compute_whitening_matrix,
+              "ms3.apply_whitening_matrix": apply_whitening_matrix, "ms3.whiten_clips": whiten_clips}
 
 
 def run(name: str, **kwargs) -> bool:

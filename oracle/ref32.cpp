@@ -393,6 +393,91 @@ void ref32_whiten_apply(const float* X, int64_t M, int64_t N, const double* WW,
     }
 }
 
+// ms3.compute_whitening_matrix (packages/ms3/p_whiten.cpp:208-298): the
+// recordings Xs[0..n_inputs) (each M x Ns[i], column-major) read as one
+// array concatenated in time (DiskReadMda32 over a file list), in chunks of
+// 1e7 timepoints (the last chunk shorter); each chunk restricted to
+// `channels` (1-based, :421-433) when n_channels > 0, float products summed in
+// a per-chunk double M2 x M2 matrix, chunk matrices added in index order (the
+// reference adds them in completion order), divided by N-1 when N > 1; then
+// whitening_matrix_from_XXt.  Returns -1 for a channel outside [1, M].
+int ref32_compute_whitening_matrix(const float* const* Xs, const int64_t* Ns, int n_inputs, int64_t M,
+                                   const int32_t* channels, int n_channels, double* W_out, double* XXt_out) {
+    const int64_t M2 = n_channels > 0 ? n_channels : M;
+    std::vector<int64_t> ch((size_t)M2);
+    for (int64_t j = 0; j < M2; j++) {
+        ch[(size_t)j] = n_channels > 0 ? (int64_t)channels[j] - 1 : j;
+        if (ch[(size_t)j] < 0 || ch[(size_t)j] >= M) return -1;
+    }
+    int64_t N = 0;
+    for (int i = 0; i < n_inputs; i++) N += Ns[i];
+    // timepoint t of the concatenation -> (input, row)
+    std::vector<int64_t> start((size_t)n_inputs + 1, 0);
+    for (int i = 0; i < n_inputs; i++) start[(size_t)i + 1] = start[(size_t)i] + Ns[i];
+    auto row = [&](int64_t t) -> const float* {
+        int i = 0;
+        while (t >= start[(size_t)i + 1]) i++;
+        return Xs[i] + (t - start[(size_t)i]) * M;
+    };
+    const int64_t processing_chunk_size = 10000000;
+    const int64_t chunk_size = N < processing_chunk_size ? N : processing_chunk_size;
+    std::vector<double> XXt((size_t)(M2 * M2), 0.0), XXt0((size_t)(M2 * M2));
+    std::vector<float> x((size_t)M2);
+    for (int64_t timepoint = 0; timepoint < N; timepoint += chunk_size) {
+        const int64_t n = std::min(chunk_size, N - timepoint);
+        std::fill(XXt0.begin(), XXt0.end(), 0.0);
+        for (int64_t i = 0; i < n; i++) {
+            const float* r = row(timepoint + i);
+            for (int64_t j = 0; j < M2; j++) x[(size_t)j] = r[ch[(size_t)j]];
+            int64_t bb = 0;
+            for (int64_t m1 = 0; m1 < M2; m1++) {
+                for (int64_t m2 = 0; m2 < M2; m2++) {
+                    float prod = x[(size_t)m1] * x[(size_t)m2];
+                    XXt0[(size_t)bb] += prod;
+                    bb++;
+                }
+            }
+        }
+        for (int64_t bb = 0; bb < M2 * M2; bb++) XXt[(size_t)bb] += XXt0[(size_t)bb];
+    }
+    if (N > 1)
+        for (int64_t ii = 0; ii < M2 * M2; ii++) XXt[(size_t)ii] /= (N - 1);
+    ref32_whitening_matrix(XXt.data(), M2, W_out, nullptr, nullptr);
+    if (XXt_out) std::memcpy(XXt_out, XXt.data(), sizeof(double) * (size_t)(M2 * M2));
+    return 0;
+}
+
+// ms3.whiten_clips (packages/ms3/p_whiten.cpp:300-345): clips M x T x L; for
+// each clip and timepoint out(m1) += x(m2) * WW[m1*M + m2] in float (the same
+// accumulation as the apply), no 1e-4 rounding (commented out there, :336-341),
+// then scale_for_quantization when quantization_unit > 0 (:445-451).
+void ref32_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* WW,
+                        double quantization_unit, float* out) {
+    for (int64_t i = 0; i < L; i++) {
+        const float* chunk_ptr = clips + i * M * T;
+        float* chunk_out_ptr = out + i * M * T;
+        for (int64_t k = 0; k < M * T; k++) chunk_out_ptr[k] = 0.f;
+        for (int64_t t = 0; t < T; t++) {
+            int64_t aa = 0;
+            const int64_t bb = M * t;
+            for (int64_t m1 = 0; m1 < M; m1++) {
+                for (int64_t m2 = 0; m2 < M; m2++) {
+                    chunk_out_ptr[bb + m1] =
+                        (float)((double)chunk_out_ptr[bb + m1] + (double)chunk_ptr[bb + m2] * WW[aa]);
+                    aa++;
+                }
+            }
+        }
+        if (quantization_unit > 0) {
+            for (int64_t k = 0; k < M * T; k++) {
+                double v = (chunk_out_ptr[k] / quantization_unit) + 0.5;
+                int iv = (v > -2147483649.0 && v < 2147483648.0) ? (int)v : INT32_MIN;
+                chunk_out_ptr[k] = (float)iv;
+            }
+        }
+    }
+}
+
 // Whole ms3.whiten on an in-memory timeseries.  Also returns XXt and W when
 // the caller passes buffers for them.
 int ref32_whiten(const float* X, int64_t M, int64_t N, double quantization_unit, int exec_threads,

@@ -52,6 +52,10 @@ def lib():
         L.ref32_whitening_matrix.argtypes = [_dp, c_i64, _dp, _dp, _dp]
         L.ref32_whiten_apply.argtypes = [_fp, c_i64, c_i64, _dp, c_dbl, c_int, _fp]
         L.ref32_whiten.argtypes = [_fp, c_i64, c_i64, c_dbl, c_int, _fp, _dp, _dp]
+        L.ref32_compute_whitening_matrix.argtypes = [ctypes.POINTER(_fp), ctypes.POINTER(c_i64), c_int, c_i64,
+                                                     ctypes.POINTER(ctypes.c_int32), c_int, _dp, _dp]
+        L.ref32_compute_whitening_matrix.restype = c_int
+        L.ref32_whiten_clips.argtypes = [_fp, c_i64, c_i64, c_i64, _dp, c_dbl, _fp]
         L.ref32_float_to_int16.argtypes = [ctypes.c_float]
         L.ref32_float_to_int16.restype = ctypes.c_int16
         _lib = L
@@ -148,3 +152,36 @@ def whiten(X_rows, quantization_unit=0.0, exec_threads=0):
     if quantization_unit > 0:
         return float_to_int16(out), C, W
     return out, C, W
+
+
+def compute_whitening_matrix(X_list, channels=None):
+    """ms3.compute_whitening_matrix on in-memory recordings: (N_i, M) float32
+    row arrays concatenated in time, optional 1-based channel numbers.
+    Returns (W, XXt) in matrix notation."""
+    arrs = [np.ascontiguousarray(X, dtype=np.float32) for X in X_list]
+    M = arrs[0].shape[1]
+    ptrs = (ctypes.POINTER(ctypes.c_float) * len(arrs))(*[_f(a) for a in arrs])
+    Ns = (ctypes.c_int64 * len(arrs))(*[a.shape[0] for a in arrs])
+    ch = np.ascontiguousarray(channels if channels is not None else [], dtype=np.int32)
+    M2 = len(ch) if len(ch) else M
+    W = np.zeros((M2, M2), np.float64)
+    C = np.zeros((M2, M2), np.float64)
+    rc = lib().ref32_compute_whitening_matrix(ptrs, Ns, len(arrs), M,
+                                              ch.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(ch),
+                                              _d(W), _d(C))
+    if rc != 0:
+        raise ValueError("channel number outside 1..M")
+    return W.T.copy(), C.T.copy()
+
+
+def whiten_clips(clips, W, quantization_unit=0.0):
+    """ms3.whiten_clips: clips as an (L, T, M) float32 array (the .mda
+    M x T x L layout); float32 out, or int16 when quantization_unit > 0."""
+    c = np.ascontiguousarray(clips, dtype=np.float32)
+    L, T, M = c.shape
+    out = np.zeros_like(c)
+    Wc = np.ascontiguousarray(np.asarray(W, dtype=np.float64).T)
+    lib().ref32_whiten_clips(_f(c), M, T, L, _d(Wc), float(quantization_unit), _f(out))
+    if quantization_unit > 0:
+        return float_to_int16(out)
+    return out

@@ -19,12 +19,13 @@ def run(*args, env=None):
     return subprocess.run([EXE, *args], capture_output=True, text=True, env=e, timeout=60)
 
 
-def test_spec_lists_the_two_processors():
+def test_spec_lists_the_processors():
     r = run("spec")
     assert r.returncode == 0
     spec = json.loads(r.stdout)
     by = {p["name"]: p for p in spec["processors"]}
-    assert set(by) == {"ms3.bandpass_filter", "ms3.whiten"}
+    assert set(by) == {"ms3.bandpass_filter", "ms3.whiten", "ms3.compute_whitening_matrix",
+                       "ms3.whiten_clips", "ms3.apply_whitening_matrix"}
     bp = by["ms3.bandpass_filter"]
     assert bp["version"] == "0.20"
     params = {p["name"]: p for p in bp["parameters"]}
@@ -36,6 +37,39 @@ def test_spec_lists_the_two_processors():
     assert bp["exe_command"].endswith("ms3.bandpass_filter $(arguments)")
     assert bp["requirements_command"].endswith("requirements ms3.bandpass_filter $(arguments)")
     assert by["ms3.whiten"]["version"] == "0.1"
+
+
+def test_spec_of_the_whitening_matrix_processors():
+    # mountainsort3_main.cpp:166-189: versions, inputs/outputs, no requirements command
+    by = {p["name"]: p for p in json.loads(run("spec").stdout)["processors"]}
+    cw = by["ms3.compute_whitening_matrix"]
+    assert cw["version"] == "0.11"
+    assert [i["name"] for i in cw["inputs"]] == ["timeseries_list"]
+    assert [o["name"] for o in cw["outputs"]] == ["whitening_matrix_out"]
+    assert cw["parameters"] == [{"description": "", "name": "channels", "optional": True}]
+    wc = by["ms3.whiten_clips"]
+    assert wc["version"] == "0.1" and [i["name"] for i in wc["inputs"]] == ["clips", "whitening_matrix"]
+    aw = by["ms3.apply_whitening_matrix"]
+    assert aw["version"] == "0.1" and [i["name"] for i in aw["inputs"]] == ["timeseries", "whitening_matrix"]
+    for p in (cw, wc, aw):
+        assert "requirements_command" not in p
+    for p in (wc, aw):
+        assert p["parameters"][0]["name"] == "quantization_unit" and p["parameters"][0]["default_value"] == 0
+
+
+def test_timeseries_list_collects_repeated_arguments(tmp_path):
+    # a repeated name is a list (clparams.cpp:55-68); recordings must agree in M
+    a, b = str(tmp_path / "a.mda"), str(tmp_path / "b.mda")
+    mdaio.writemda(np.zeros((4, 50), np.float32), a)
+    mdaio.writemda(np.zeros((5, 50), np.float32), b)
+    out = str(tmp_path / "w.mda")
+    r = run("ms3.compute_whitening_matrix", f"--timeseries_list={a}", f"--timeseries_list={b}",
+            f"--whitening_matrix_out={out}")
+    assert r.returncode == 255 and "channel count" in r.stderr and not os.path.exists(out)
+    # channel numbers are 1-based; 0 (or a non-number) is rejected before any device work
+    r = run("ms3.compute_whitening_matrix", f"--timeseries_list={a}", "--channels=1,0",
+            f"--whitening_matrix_out={out}")
+    assert r.returncode == 255 and "outside 1..4" in r.stderr and not os.path.exists(out)
 
 
 def test_spec_single_and_unknown():

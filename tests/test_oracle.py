@@ -194,3 +194,38 @@ def test_float_to_int16_x86(ref32):
     v = np.array([1.9, -1.9, 32767.5, 32768.0, -32769.0, 70000.0, 3e9, np.nan], np.float32)
     got = ref32.float_to_int16(v)
     np.testing.assert_array_equal(got, np.array([1, -1, 32767, -32768, 32767, 4464, 0, 0], np.int16))
+
+
+def test_compute_whitening_matrix_oracle_concatenates_and_selects_channels(ref32):
+    # ms3.compute_whitening_matrix (p_whiten.cpp:208-298): recordings concatenated
+    # in time, 1-based channel subset, XXt / (N - 1), then the power-iteration W
+    from mountainsort_b200 import synth
+    A = synth.generate_numpy(12, 30000, K=6, seed=3)
+    B = synth.generate_numpy(12, 17001, K=6, seed=4)
+    ch = [3, 1, 12, 7]
+    W, C = ref32.compute_whitening_matrix([A, B], channels=ch)
+    X = np.concatenate([A, B])[:, [c - 1 for c in ch]].astype(np.float64)
+    assert o64.rel_l2(C, X.T @ X / (X.shape[0] - 1)) <= 1e-9
+    W64 = o64.whitening_matrix(C)
+    W64 = W64[0] if isinstance(W64, tuple) else W64
+    assert o64.rel_l2(W, W64) <= 1e-12
+    # no subset = all channels, and the same XXt as ms3.whiten's pass 1 on the concatenation
+    W_all, C_all = ref32.compute_whitening_matrix([A, B])
+    assert o64.rel_l2(C_all, ref32.whiten_xxt(np.concatenate([A, B]))) <= 1e-12
+    with pytest.raises(ValueError):
+        ref32.compute_whitening_matrix([A], channels=[0])
+
+
+def test_whiten_clips_oracle_has_no_1e4_rounding(ref32):
+    rng = np.random.default_rng(5)
+    clips = rng.standard_normal((20, 40, 12)).astype(np.float32)
+    A = rng.standard_normal((12, 12))
+    W = (A + A.T) / 24
+    out = ref32.whiten_clips(clips, W)
+    exact = np.einsum("ltm,mk->ltk", clips.astype(np.float64), W)  # out(m1) = sum_m2 x(m2) W(m2, m1)
+    assert o64.rel_l2(out, exact) <= 1e-6
+    assert np.abs(out * 1e4 - np.round(out * 1e4)).max() > 1e-2  # not multiples of 1e-4
+    q = 0.5
+    out16 = ref32.whiten_clips(clips, W, quantization_unit=q)
+    assert out16.dtype == np.int16
+    assert np.abs(out16.astype(np.float64) - np.trunc(out.astype(np.float64) / q + 0.5)).max() <= 1
