@@ -119,6 +119,15 @@ MS3GPU_API int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_
 MS3GPU_API int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
                   const ms3gpu_whiten_opts* opts, void* stream);
 
+/* ms3.bandpass_filter on an int16 recording (an int16 .mda input), read
+ * as the reference's reader converts it (mda/mdaio.cpp:205-230, int16 ->
+ * float) -- here inside the filter's loads, so the int16 array is what
+ * crosses PCIe and HBM.  Otherwise as ms3gpu_bandpass_filter; with
+ * freq_max == 0 the output is an int16 copy of the input (the reference
+ * copies the file). */
+MS3GPU_API int ms3gpu_bandpass_filter_i16(const int16_t* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                                          const ms3gpu_bandpass_opts* opts, void* stream);
+
 /* The two processors back to back as mountainsort3.mlp runs them
  * (ms3.bandpass_filter then ms3.whiten), sharing device buffers.
  * filt_out (the bandpass output, float32 M x N) may be NULL when the caller

@@ -73,6 +73,7 @@ SIGNATURES = {
     "ms3gpu_whiten_covariance_noalloc": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
     "ms3gpu_whitening_matrix": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
+    "ms3gpu_bandpass_filter_i16": (ctypes.c_int, [_vp, _i64, _i64, _vp, ctypes.POINTER(BandpassOpts), _vp]),
     "ms3gpu_compute_whitening_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _i64, _vp, ctypes.c_int32, _vp,
                                                        _vp]),
     "ms3gpu_whiten_clips": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),

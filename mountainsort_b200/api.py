@@ -97,9 +97,14 @@ def bandpass_filter(X, samplerate, freq_min, freq_max, freq_wid=1000.0, quantiza
                     subsample_factor=1, num_threads=None, out=None, stream=None):
     """ms3.bandpass_filter (packages/ms3/p_bandpass_filter.cpp:115-229) on an
     (N, M) array; returns (N // subsample_factor, M) float32, or int16 when
-    quantization_unit != 0."""
+    quantization_unit != 0.  An int16 array is filtered as the reference
+    reads an int16 file (converted to float), without a float copy of it."""
     L = _lib.load()
-    X = _as_f32_rows(X)
+    i16 = (_is_torch(X) and X.dtype == torch.int16) or (not _is_torch(X) and np.asarray(X).dtype == np.int16)
+    if i16:
+        X = X.contiguous() if _is_torch(X) else np.ascontiguousarray(X)
+    else:
+        X = _as_f32_rows(X)
     N, M = X.shape
     o = bandpass_opts(samplerate, freq_min, freq_max, freq_wid, quantization_unit, subsample_factor,
                       num_threads)
@@ -107,8 +112,10 @@ def bandpass_filter(X, samplerate, freq_min, freq_max, freq_wid=1000.0, quantiza
     check(L.ms3gpu_bandpass_output_dims(M, N, ctypes.byref(o), ctypes.byref(Mo), ctypes.byref(No),
                                         ctypes.byref(dt)))
     if out is None:
-        out = _empty_like(X, (No.value, Mo.value), np.int16 if dt.value == _lib.DTYPE_INT16 else np.float32)
-    check(L.ms3gpu_bandpass_filter(_ptr(X), M, N, _ptr(out), ctypes.byref(o), _stream_ptr(X, stream)))
+        out_i16 = dt.value == _lib.DTYPE_INT16 or (i16 and float(freq_max) == 0)
+        out = _empty_like(X, (No.value, Mo.value), np.int16 if out_i16 else np.float32)
+    fn = L.ms3gpu_bandpass_filter_i16 if i16 else L.ms3gpu_bandpass_filter
+    check(fn(_ptr(X), M, N, _ptr(out), ctypes.byref(o), _stream_ptr(X, stream)))
     return out
 
 

@@ -67,16 +67,26 @@ struct Geom {
     int64_t N2;          // output timepoints
     int out_i16;
     double qscale;       // 1 / quantization_unit
+    int in_i16;          // raw is int16 (converted to float on load, like the reference's reader)
 };
 
 // ---------------------------------------------------------------- kernels
 
-__device__ __forceinline__ float2 load_signal(const float* __restrict__ raw, const Geom& g, int64_t t,
-                                              int64_t s) {
+__device__ __forceinline__ float2 load_signal(const void* __restrict__ raw, const Geom& g, int64_t t, int64_t s) {
     if (t < 0 || t >= g.N || s >= g.P) return make_float2(0.f, 0.f);
-    const float* row = raw + t * g.M;
+    const int64_t m0 = g.paired ? 2 * s : s;
+    if (g.in_i16) {
+        // int16 -> float as mdaReadData converts (mda/mdaio.cpp:205-230)
+        const int16_t* row = static_cast<const int16_t*>(raw) + t * g.M;
+        if (!g.paired) return make_float2((float)row[s], 0.f);
+        if (g.m_even) {
+            const short2 v = *reinterpret_cast<const short2*>(row + m0);
+            return make_float2((float)v.x, (float)v.y);
+        }
+        return make_float2((float)row[m0], (m0 + 1 < g.M) ? (float)row[m0 + 1] : 0.f);
+    }
+    const float* row = static_cast<const float*>(raw) + t * g.M;
     if (!g.paired) return make_float2(row[s], 0.f);
-    const int64_t m0 = 2 * s;
     if (g.m_even) return *reinterpret_cast<const float2*>(row + m0);
     return make_float2(row[m0], (m0 + 1 < g.M) ? row[m0 + 1] : 0.f);
 }
@@ -102,7 +112,7 @@ __device__ __forceinline__ void load_plan(SubFft& dst, const SubFft& src) {
 }
 
 // F1: forward L1-point transforms of the window columns.
-__global__ void __launch_bounds__(kThreads) bp_cols_forward(const float* __restrict__ raw,
+__global__ void __launch_bounds__(kThreads) bp_cols_forward(const void* __restrict__ raw,
                                                             float2* __restrict__ scratch, Geom g,
                                                             SubFft P1, const float2* __restrict__ tw1,
                                                             int64_t unit0) {
@@ -293,7 +303,7 @@ __device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geo
 
 // F1, forward columns of length L1 = RA * RB.
 template <int RA, int RB>
-__global__ void __launch_bounds__(256, 3) bpr_cols_forward(const float* __restrict__ raw, float2* __restrict__ scratch,
+__global__ void __launch_bounds__(256, 3) bpr_cols_forward(const void* __restrict__ raw, float2* __restrict__ scratch,
                                                         Geom g, const float2* __restrict__ roots, int64_t unit0) {
     constexpr int n = RA * RB;
     extern __shared__ float4 smem_f4[];
@@ -311,10 +321,20 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_forward(const float* __restri
         const int gi = it & (G - 1), i = it >> g.log2G;
         float2 u[RA];
         if (interior) {
-            const float2* p = reinterpret_cast<const float2*>(raw + (t0 + (int64_t)i * g.L2) * g.M) + (s0 + gi);
-            const int64_t step = (int64_t)RB * g.L2 * (g.M / 2);  // float2 per RB window rows
+            const int64_t row0 = (t0 + (int64_t)i * g.L2) * g.M;
+            const int64_t step = (int64_t)RB * g.L2 * (g.M / 2);  // pairs per RB window rows
+            if (g.in_i16) {
+                const short2* p = reinterpret_cast<const short2*>(static_cast<const int16_t*>(raw) + row0) + (s0 + gi);
 #pragma unroll
-            for (int q = 0; q < RA; q++) u[q] = __ldg(p + q * step);
+                for (int q = 0; q < RA; q++) {
+                    const short2 v = __ldg(p + q * step);
+                    u[q] = make_float2((float)v.x, (float)v.y);
+                }
+            } else {
+                const float2* p = reinterpret_cast<const float2*>(static_cast<const float*>(raw) + row0) + (s0 + gi);
+#pragma unroll
+                for (int q = 0; q < RA; q++) u[q] = __ldg(p + q * step);
+            }
         } else {
 #pragma unroll
             for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * g.L2, s0 + gi);
@@ -847,8 +867,8 @@ int64_t bandpass_chunk_size(int64_t M, int64_t num_threads) {
     return chunk_size;
 }
 
-void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
-                     cudaStream_t stream, int64_t c_begin, int64_t c_end) {
+void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
+                     cudaStream_t stream, int64_t c_begin, int64_t c_end, bool in_i16) {
     const int sub = bp.subsample_factor ? bp.subsample_factor : 1;
     if (sub < 1) throw_invalid("subsample_factor must be >= 1");
     const int64_t N2 = N / sub;
@@ -856,7 +876,8 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     if (bp.freq_max == 0) {
         // p_bandpass_filter.cpp:117-119: the input file is copied unchanged.
         if (M * N > 0)
-            MS3_CUDA(cudaMemcpyAsync(out, raw, sizeof(float) * (size_t)(M * N), cudaMemcpyDeviceToDevice, stream));
+            MS3_CUDA(cudaMemcpyAsync(out, raw, (in_i16 ? 2 : 4) * (size_t)(M * N), cudaMemcpyDeviceToDevice,
+                                     stream));
         return;
     }
     if (M <= 0 || N2 <= 0) return;
@@ -870,8 +891,10 @@ void bandpass_device(const float* raw, int64_t M, int64_t N, void* out, const Ba
     g.N = N;
     g.paired = plan->paired;
     g.P = g.paired ? (M + 1) / 2 : M;
-    // float2 loads/stores need even M and 8-byte aligned caller buffers
-    g.m_even = (M % 2 == 0) && ((uintptr_t)raw % 8 == 0) && ((uintptr_t)out % 8 == 0);
+    // pair loads (float2, or short2 for int16 input) and float2 stores need
+    // even M and aligned caller buffers
+    g.in_i16 = in_i16 ? 1 : 0;
+    g.m_even = (M % 2 == 0) && ((uintptr_t)raw % (in_i16 ? 4 : 8) == 0) && ((uintptr_t)out % 8 == 0);
     g.L = L;
     g.L1 = plan->L1;
     g.L2 = plan->L2;

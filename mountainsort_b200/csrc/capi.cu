@@ -255,28 +255,39 @@ int ms3gpu_whiten_requirements(int64_t M, int64_t N, double* peak_ram_mb) {
     });
 }
 
+namespace {
+void bandpass_any(const void* timeseries, bool in_i16, int64_t M, int64_t N, void* timeseries_out,
+                  const ms3gpu_bandpass_opts* opts, void* stream) {
+    check_shape(M, N);
+    BandpassParams p = to_params(opts);
+    cudaStream_t s = as_stream(stream);
+    const bool copy = p.freq_max == 0;
+    const int64_t N2 = copy ? N : N / p.subsample_factor;
+    const size_t in_esz = in_i16 ? 2 : 4;
+    const size_t esz = copy ? in_esz : (p.quantization_unit != 0 ? 2 : 4);
+    const size_t in_bytes = in_esz * (size_t)(M * N);
+    const size_t out_bytes = esz * (size_t)(M * N2);
+    require(timeseries, "timeseries", in_bytes > 0);
+    require(timeseries_out, "timeseries_out", out_bytes > 0);
+    InView in;
+    stage_in(in, timeseries, in_bytes, s);
+    OutView out;
+    out.setup(timeseries_out, out_bytes, s);
+    bandpass_device(in.ptr, M, N, out.ptr, p, s, 0, -1, in_i16);
+    out.finish(s);
+    MS3_CUDA(cudaStreamSynchronize(s));
+    bandpass_check_timeout(s);
+}
+}  // namespace
+
 int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
                            const ms3gpu_bandpass_opts* opts, void* stream) {
-    return guarded([&] {
-        check_shape(M, N);
-        BandpassParams p = to_params(opts);
-        cudaStream_t s = as_stream(stream);
-        const bool copy = p.freq_max == 0;
-        const int64_t N2 = copy ? N : N / p.subsample_factor;
-        const size_t esz = (!copy && p.quantization_unit != 0) ? 2 : 4;
-        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
-        const size_t out_bytes = esz * (size_t)(M * N2);
-        require(timeseries, "timeseries", in_bytes > 0);
-        require(timeseries_out, "timeseries_out", out_bytes > 0);
-        InView in;
-        stage_in(in, timeseries, in_bytes, s);
-        OutView out;
-        out.setup(timeseries_out, out_bytes, s);
-        bandpass_device(static_cast<const float*>(in.ptr), M, N, out.ptr, p, s);
-        out.finish(s);
-        MS3_CUDA(cudaStreamSynchronize(s));
-        bandpass_check_timeout(s);
-    });
+    return guarded([&] { bandpass_any(timeseries, false, M, N, timeseries_out, opts, stream); });
+}
+
+int ms3gpu_bandpass_filter_i16(const int16_t* timeseries, int64_t M, int64_t N, void* timeseries_out,
+                               const ms3gpu_bandpass_opts* opts, void* stream) {
+    return guarded([&] { bandpass_any(timeseries, true, M, N, timeseries_out, opts, stream); });
 }
 
 int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt, void* stream) {

@@ -1,7 +1,10 @@
 // .mda file I/O for the ms3gpu.mp processor executable (see mdaio.h).
 #include "mdaio.h"
 
+#include <dirent.h>
 #include <sys/stat.h>
+
+#include <algorithm>
 
 #include <cstdio>
 #include <cstring>
@@ -22,6 +25,11 @@ void convert(const S* src, D* dst, int64_t n) {
     for (int64_t i = 0; i < n; i++) dst[i] = (D)src[i];
 }
 }  // namespace
+
+bool is_directory(const std::string& path) {
+    struct stat st;
+    return stat(path.c_str(), &st) == 0 && S_ISDIR(st.st_mode);
+}
 
 int bytes_per_entry(int32_t t) {
     switch (t) {
@@ -67,9 +75,8 @@ static bool read_header_file(FILE* f, MdaHeader& h, std::string& err) {
 }
 
 bool read_header(const std::string& path, MdaHeader& h, std::string& err) {
-    struct stat st;
-    if (stat(path.c_str(), &st) == 0 && S_ISDIR(st.st_mode)) {
-        err = "directory (concatenated) inputs are not supported: " + path;
+    if (is_directory(path)) {
+        err = "expected an .mda file, got a directory: " + path;
         return false;
     }
     FilePtr f(std::fopen(path.c_str(), "rb"));
@@ -244,6 +251,112 @@ bool write_array(const std::string& path, int32_t data_type, const std::vector<i
         err = "cannot rename " + tmp + " to " + path;
         return false;
     }
+    return true;
+}
+
+}  // namespace ms3io
+
+namespace ms3io {
+
+// DiskReadMda32Private::find_all_mda_files_in_directory (recursive), mda/
+// diskreadmda32.cpp:896-913: the directory's files ending in ".mda", sorted
+// by name (QDir::Name: case-sensitive code-point order), then for every
+// subdirectory (sorted) the files of `dir_path + "/dirname"` -- the
+// reference appends the literal text "dirname", not the subdirectory's
+// name, and that is kept.
+void concat_directory_files(const std::string& dir, std::vector<std::string>& out) {
+    std::vector<std::string> files, dirs;
+    if (DIR* d = opendir(dir.c_str())) {
+        while (dirent* e = readdir(d)) {
+            const std::string n = e->d_name;
+            if (n == "." || n == "..") continue;
+            struct stat st;
+            if (stat((dir + "/" + n).c_str(), &st) != 0) continue;
+            if (S_ISDIR(st.st_mode))
+                dirs.push_back(n);
+            else if (S_ISREG(st.st_mode) && n.size() >= 4 && n.compare(n.size() - 4, 4, ".mda") == 0)
+                files.push_back(n);
+        }
+        closedir(d);
+    }
+    std::sort(files.begin(), files.end());
+    std::sort(dirs.begin(), dirs.end());
+    for (const std::string& n : files) out.push_back(dir + "/" + n);
+    for (size_t i = 0; i < dirs.size(); i++) concat_directory_files(dir + "/dirname", out);
+}
+
+bool input_files(const std::string& path, std::vector<std::string>& files, std::string& err) {
+    files.clear();
+    if (!is_directory(path)) {
+        files.push_back(path);
+        return true;
+    }
+    concat_directory_files(path, files);
+    if (files.empty()) {
+        err = "no .mda files in directory " + path;
+        return false;
+    }
+    return true;
+}
+
+bool read_dims_any(const std::string& path, int64_t& M, int64_t& N, int32_t& data_type, std::string& err) {
+    std::vector<std::string> files;
+    if (!input_files(path, files, err)) return false;
+    M = -1;
+    N = 0;
+    for (const std::string& f : files) {
+        MdaHeader h;
+        if (!read_header(f, h, err)) return false;
+        const int64_t m = h.dims[0], n = h.dims.size() > 1 ? h.dims[1] : 1;
+        if (M >= 0 && m != M) {
+            err = "the files of " + path + " differ in channel count";
+            return false;
+        }
+        data_type = (M < 0 || data_type == h.data_type) ? h.data_type : 0;  // 0: mixed types
+        M = m;
+        N += n;
+    }
+    return true;
+}
+
+bool read_timeseries_any_f32(const std::string& path, int64_t& M, int64_t& N, std::vector<float>& data,
+                             std::string& err) {
+    std::vector<std::string> files;
+    if (!input_files(path, files, err)) return false;
+    if (files.size() == 1) return read_timeseries_f32(files[0], M, N, data, err);
+    M = -1;
+    N = 0;
+    data.clear();
+    std::vector<float> part;
+    for (const std::string& f : files) {
+        int64_t m = 0, n = 0;
+        if (!read_timeseries_f32(f, m, n, part, err)) return false;
+        if (M >= 0 && m != M) {
+            err = "the files of " + path + " differ in channel count";
+            return false;
+        }
+        M = m;
+        N += n;
+        data.insert(data.end(), part.begin(), part.end());  // column-major M x n: append in time
+    }
+    return true;
+}
+
+bool read_timeseries_i16(const std::string& path, int64_t& M, int64_t& N, std::vector<int16_t>& data,
+                         std::string& err) {
+    MdaHeader h;
+    if (!read_header(path, h, err)) return false;
+    if (h.data_type != kInt16) {
+        err = path + " is not int16";
+        return false;
+    }
+    FilePtr f(std::fopen(path.c_str(), "rb"));
+    if (!f) { err = "cannot open " + path; return false; }
+    std::fseek(f.get(), (long)h.header_size, SEEK_SET);
+    M = h.dims[0];
+    N = h.dims.size() > 1 ? h.dims[1] : 1;
+    data.resize((size_t)(M * N));
+    if ((int64_t)std::fread(data.data(), 2, (size_t)(M * N), f.get()) != M * N) { err = "short read from " + path; return false; }
     return true;
 }
 

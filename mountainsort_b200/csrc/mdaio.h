@@ -47,6 +47,20 @@ bool read_array_f64(const std::string& path, std::vector<int64_t>& dims, std::ve
 bool write_array(const std::string& path, int32_t data_type, const std::vector<int64_t>& dims, const void* data,
                  std::string& err);
 
+bool is_directory(const std::string& path);
+
+// A timeseries input as the reference's DiskReadMda32 opens it
+// (mda/diskreadmda32.cpp:234-237, 283-288): a file, or a directory whose
+// .mda files are concatenated along time.
+bool input_files(const std::string& path, std::vector<std::string>& files, std::string& err);
+// M, total N and the common data type (0 when the files' types differ).
+bool read_dims_any(const std::string& path, int64_t& M, int64_t& N, int32_t& data_type, std::string& err);
+bool read_timeseries_any_f32(const std::string& path, int64_t& M, int64_t& N, std::vector<float>& data,
+                             std::string& err);
+// An int16 file's entries as they are (no conversion).
+bool read_timeseries_i16(const std::string& path, int64_t& M, int64_t& N, std::vector<int16_t>& data,
+                         std::string& err);
+
 // Byte copy that, like QFile::copy, refuses to overwrite an existing file.
 bool copy_file(const std::string& src, const std::string& dst, std::string& err);
 

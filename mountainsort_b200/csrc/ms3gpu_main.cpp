@@ -214,15 +214,16 @@ int run_bandpass(const CLParams& clp, bool requirements_only) {
     const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
     ms3gpu_bandpass_opts o = bandpass_opts(clp);
     std::string err;
-    ms3io::MdaHeader h;
     if (o.freq_max == 0 && !requirements_only) {
-        // p_bandpass_filter.cpp:117-119
+        // p_bandpass_filter.cpp:117-119 (QFile::copy, which cannot copy a directory)
+        if (ms3io::is_directory(in)) return fail("cannot copy a directory: " + in);
         if (!ms3io::copy_file(in, out, err)) return fail(err);
         return 0;
     }
-    if (!ms3io::read_header(in, h, err)) return fail(err);
-    const int64_t M = h.dims[0];
-    const int64_t N = h.dims.size() > 1 ? h.dims[1] : 1;
+    // a file, or a directory of .mda files concatenated in time (:128-131)
+    int64_t M = 0, N = 0;
+    int32_t dtype = 0;
+    if (!ms3io::read_dims_any(in, M, N, dtype, err)) return fail(err);
     if (requirements_only) {
         double mb = 0;
         if (ms3gpu_bandpass_requirements(M, N, &o, &mb) != MS3GPU_OK) {
@@ -232,17 +233,26 @@ int run_bandpass(const CLParams& clp, bool requirements_only) {
         print_requirements(mb);
         return 0;
     }
-    std::vector<float> X;
-    int64_t M1 = 0, N1 = 0;
-    if (!ms3io::read_timeseries_f32(in, M1, N1, X, err)) return fail(err);
     int64_t Mo = 0, No = 0;
     int32_t dt = 0;
     if (ms3gpu_bandpass_output_dims(M, N, &o, &Mo, &No, &dt) != MS3GPU_OK) return fail(ms3gpu_last_error());
     std::vector<unsigned char> Y((size_t)(Mo * No) * (dt == MS3GPU_DTYPE_INT16 ? 2 : 4));
     std::fprintf(stderr, "ms3gpu: bandpass %lld x %lld, chunk %lld (T=%d)\n", (long long)M, (long long)N,
                  (long long)ms3gpu_bandpass_chunk_size(M, o.num_threads), o.num_threads);
-    if (ms3gpu_bandpass_filter(X.data(), M, N, Y.data(), &o, nullptr) != MS3GPU_OK)
-        return fail(ms3gpu_last_error());
+    int rc;
+    if (dtype == ms3io::kInt16 && !ms3io::is_directory(in)) {
+        // an int16 recording goes to the GPU as int16 and is converted in the filter's loads
+        std::vector<int16_t> X16;
+        int64_t M1 = 0, N1 = 0;
+        if (!ms3io::read_timeseries_i16(in, M1, N1, X16, err)) return fail(err);
+        rc = ms3gpu_bandpass_filter_i16(X16.data(), M, N, Y.data(), &o, nullptr);
+    } else {
+        std::vector<float> X;
+        int64_t M1 = 0, N1 = 0;
+        if (!ms3io::read_timeseries_any_f32(in, M1, N1, X, err)) return fail(err);
+        rc = ms3gpu_bandpass_filter(X.data(), M, N, Y.data(), &o, nullptr);
+    }
+    if (rc != MS3GPU_OK) return fail(ms3gpu_last_error());
     if (!ms3io::write_timeseries(out, dt, Mo, No, Y.data(), err)) return fail(err);
     return 0;
 }
@@ -253,10 +263,9 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
     o.quantization_unit = clp.num("quantization_unit", 0);  // mountainsort3_main.cpp:576
     o.precision = precision_of(clp);
     std::string err;
-    ms3io::MdaHeader h;
-    if (!ms3io::read_header(in, h, err)) return fail(err);
-    const int64_t M = h.dims[0];
-    const int64_t N = h.dims.size() > 1 ? h.dims[1] : 1;
+    int64_t M = 0, N = 0;
+    int32_t dtype = 0;
+    if (!ms3io::read_dims_any(in, M, N, dtype, err)) return fail(err);
     if (requirements_only) {
         double mb = 0;
         if (ms3gpu_whiten_requirements(M, N, &mb) != MS3GPU_OK) {
@@ -268,7 +277,7 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
     }
     std::vector<float> X;
     int64_t M1 = 0, N1 = 0;
-    if (!ms3io::read_timeseries_f32(in, M1, N1, X, err)) return fail(err);
+    if (!ms3io::read_timeseries_any_f32(in, M1, N1, X, err)) return fail(err);
     const bool i16 = o.quantization_unit > 0;
     std::vector<unsigned char> Y((size_t)(M * N) * (i16 ? 2 : 4));
     if (ms3gpu_whiten(X.data(), M, N, Y.data(), &o, nullptr) != MS3GPU_OK) return fail(ms3gpu_last_error());
@@ -313,7 +322,7 @@ int run_compute_whitening_matrix(const CLParams& clp) {
     std::string err;
     for (size_t i = 0; i < it->second.size(); i++) {
         int64_t Mi = 0, Ni = 0;
-        if (!ms3io::read_timeseries_f32(it->second[i], Mi, Ni, data[i], err)) return fail(err);
+        if (!ms3io::read_timeseries_any_f32(it->second[i], Mi, Ni, data[i], err)) return fail(err);
         if (M >= 0 && Mi != M) return fail("the recordings of timeseries_list differ in channel count");
         M = Mi;
         ptrs.push_back(data[i].data());
@@ -337,7 +346,7 @@ int run_apply_whitening_matrix(const CLParams& clp) {
     std::string err;
     std::vector<float> X;
     int64_t M = 0, N = 0;
-    if (!ms3io::read_timeseries_f32(in, M, N, X, err)) return fail(err);
+    if (!ms3io::read_timeseries_any_f32(in, M, N, X, err)) return fail(err);
     std::vector<double> W;
     if (!read_whitening_matrix(wpath, M, W, err)) return fail(err);
     const bool i16 = q > 0;

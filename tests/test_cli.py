@@ -121,3 +121,30 @@ def test_freq_max_zero_copies_file(tmp_path):
     # QFile::copy semantics: an existing destination is not overwritten
     r = run("ms3.bandpass_filter", f"--timeseries={src}", f"--timeseries_out={out}", "--freq_max=0")
     assert r.returncode == 255
+
+
+def test_directory_input_is_concatenated_like_diskreadmda32(tmp_path, ref32):
+    # mda/diskreadmda32.cpp:283-288, 896-913: the directory's .mda files sorted by
+    # name; subdirectories are looked up as <dir>/dirname (kept as the reference has it)
+    d = tmp_path / "rec"
+    d.mkdir()
+    mdaio.writemda(np.zeros((4, 30), np.float32), str(d / "b.mda"))
+    mdaio.writemda(np.zeros((4, 20), np.float32), str(d / "a.mda"))
+    (d / "notes.txt").write_text("not an mda")
+    sub = d / "sub"
+    sub.mkdir()
+    mdaio.writemda(np.zeros((5, 10), np.float32), str(sub / "c.mda"))  # skipped: not <dir>/dirname
+    r = run("requirements", "ms3.whiten", f"--timeseries={d}", "--timeseries_out=o.mda")
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout)["peak_ram_mb"] == pytest.approx(ref32.lib().ref32_whiten_peak_ram_mb(4))
+    # a subdirectory literally named "dirname" is read, once per subdirectory
+    dn = d / "dirname"
+    dn.mkdir()
+    mdaio.writemda(np.zeros((6, 10), np.float32), str(dn / "x.mda"))
+    r = run("requirements", "ms3.whiten", f"--timeseries={d}", "--timeseries_out=o.mda")
+    assert r.returncode == 255 and "differ in channel count" in r.stderr
+    # freq_max = 0 copies with QFile::copy, which cannot copy a directory
+    out = str(tmp_path / "copy.mda")
+    r = run("ms3.bandpass_filter", f"--timeseries={d}", f"--timeseries_out={out}", "--samplerate=30000",
+            "--freq_min=300", "--freq_max=0")
+    assert r.returncode == 255 and not os.path.exists(out)
