@@ -138,6 +138,27 @@ MS3GPU_API int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_
                            void* pre_out, const ms3gpu_bandpass_opts* bp,
                            const ms3gpu_whiten_opts* wh, void* stream);
 
+/* One recording of a batch: ms3.bandpass_filter then ms3.whiten, as
+ * ms3gpu_bandpass_whiten (same buffer rules).  `status` receives the job's
+ * result. */
+typedef struct ms3gpu_job {
+    const float* timeseries; /* M x N float32, host or device */
+    int64_t M, N;
+    float* filt_out;         /* optional, M x N float32 */
+    void* pre_out;           /* M x N float32, int16 when wh.quantization_unit > 0 */
+    ms3gpu_bandpass_opts bp; /* subsample_factor 1, quantization_unit 0 */
+    ms3gpu_whiten_opts wh;
+    int32_t status;          /* out: MS3GPU_OK or the job's error code */
+} ms3gpu_job;
+
+/* A batch of recordings of any sizes (no counterpart in the reference, which
+ * runs one processor call per recording): the jobs run concurrently on a
+ * few internal streams ordered after `stream`, so small recordings share
+ * the GPU.  Outputs are those of n_jobs separate ms3gpu_bandpass_whiten
+ * calls.  Returns MS3GPU_OK when every job succeeded, else the first failing
+ * job's code (ms3gpu_last_error() names the job). */
+MS3GPU_API int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream);
+
 /* Stage: whiten pass 1 (p_whiten.cpp:64-118).  XXt = sum_t x_t x_t^T,
  * divided by N-1 when N > 1, M x M doubles. */
 MS3GPU_API int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt,

@@ -43,6 +43,20 @@ class WhitenOpts(ctypes.Structure):
     _fields_ = [("quantization_unit", ctypes.c_double), ("precision", ctypes.c_int32)]
 
 
+class Job(ctypes.Structure):
+    """ms3gpu_job: one recording of ms3gpu_bandpass_whiten_batch."""
+    _fields_ = [
+        ("timeseries", ctypes.c_void_p),
+        ("M", ctypes.c_int64),
+        ("N", ctypes.c_int64),
+        ("filt_out", ctypes.c_void_p),
+        ("pre_out", ctypes.c_void_p),
+        ("bp", BandpassOpts),
+        ("wh", WhitenOpts),
+        ("status", ctypes.c_int32),
+    ]
+
+
 class Ms3GpuError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"ms3gpu error {code}: {msg}")
@@ -74,6 +88,7 @@ SIGNATURES = {
     "ms3gpu_whitening_matrix": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "ms3gpu_apply_whitening_matrix": (ctypes.c_int, [_vp, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
     "ms3gpu_bandpass_filter_i16": (ctypes.c_int, [_vp, _i64, _i64, _vp, ctypes.POINTER(BandpassOpts), _vp]),
+    "ms3gpu_bandpass_whiten_batch": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_int32, _vp]),
     "ms3gpu_compute_whitening_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _i64, _vp, ctypes.c_int32, _vp,
                                                        _vp]),
     "ms3gpu_whiten_clips": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),

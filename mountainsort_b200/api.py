@@ -155,6 +155,36 @@ def bandpass_whiten(X, samplerate, freq_min, freq_max, freq_wid=1000.0, num_thre
     return (filt_out, out) if filt_out is not None else out
 
 
+def bandpass_whiten_batch(recordings, stream=None, precision="plain"):
+    """Many recordings through ms3.bandpass_filter + ms3.whiten at once
+    (ms3gpu_bandpass_whiten_batch): `recordings` is a list of dicts with keys
+    X ((N, M) array) and samplerate, freq_min, freq_max, optional freq_wid,
+    num_threads, quantization_unit (of the whiten step).  Returns the list of
+    whitened outputs; raises on the first failing job after all have run."""
+    L = _lib.load()
+    jobs = (_lib.Job * len(recordings))()
+    keep = []
+    outs = []
+    for k, r in enumerate(recordings):
+        X = _as_f32_rows(r["X"])
+        N, M = X.shape
+        q = float(r.get("quantization_unit", 0.0))
+        out = _empty_like(X, (N, M), np.int16 if q > 0 else np.float32)
+        keep.append(X)
+        outs.append(out)
+        j = jobs[k]
+        j.timeseries = _ptr(X)
+        j.M, j.N = M, N
+        j.filt_out = None
+        j.pre_out = _ptr(out)
+        j.bp = bandpass_opts(r["samplerate"], r["freq_min"], r["freq_max"], r.get("freq_wid", 1000.0), 0.0, 1,
+                             r.get("num_threads"))
+        j.wh = WhitenOpts(q, _PRECISION[precision])
+    s = _stream_ptr(keep[0], stream) if keep else 0
+    check(L.ms3gpu_bandpass_whiten_batch(jobs, len(recordings), s))
+    return outs
+
+
 def whiten_covariance(X, stream=None):
     """XXt = sum_t x_t x_t^T / (N-1) (p_whiten.cpp:64-118), M x M float64."""
     L = _lib.load()

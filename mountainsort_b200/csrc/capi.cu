@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -288,6 +289,120 @@ int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* 
 int ms3gpu_bandpass_filter_i16(const int16_t* timeseries, int64_t M, int64_t N, void* timeseries_out,
                                const ms3gpu_bandpass_opts* opts, void* stream) {
     return guarded([&] { bandpass_any(timeseries, true, M, N, timeseries_out, opts, stream); });
+}
+
+namespace {
+// Device state of one batch job between its compute and its copy-back.
+struct BatchJob {
+    cudaStream_t s = nullptr;
+    InView in;
+    OutView filt, pre;
+    DevBuf filt_own, mats, err;
+};
+
+// Issues one job's device work on js (no copy back, no synchronisation).
+void issue_batch_job(const ms3gpu_job& j, BatchJob& st) {
+    check_shape(j.M, j.N);
+    BandpassParams p = to_params(&j.bp);
+    if (p.subsample_factor != 1 || p.quantization_unit != 0)
+        throw_invalid("bandpass_whiten needs subsample_factor 1 and quantization_unit 0");
+    const int64_t M = j.M, N = j.N;
+    const double q = j.wh.quantization_unit;
+    const bool mixed = check_precision(j.wh.precision);
+    const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+    const size_t pre_bytes = (q > 0 ? 2 : 4) * (size_t)(M * N);
+    require(j.timeseries, "timeseries", in_bytes > 0);
+    require(j.pre_out, "pre_out", pre_bytes > 0);
+    cudaStream_t s = st.s;
+    stage_in(st.in, j.timeseries, in_bytes, s);
+    float* filt_d = nullptr;
+    if (j.filt_out) {
+        st.filt.setup(j.filt_out, in_bytes, s);
+        filt_d = static_cast<float*>(st.filt.ptr);
+    } else if (in_bytes) {
+        st.filt_own.alloc(in_bytes, s);
+        filt_d = st.filt_own.as<float>();
+    }
+    bandpass_device(static_cast<const float*>(st.in.ptr), M, N, filt_d, p, s);
+    st.pre.setup(j.pre_out, pre_bytes, s);
+    st.mats.alloc(sizeof(double) * (size_t)(2 * M * M), s);
+    double* XXt = st.mats.as<double>();
+    double* W = XXt + M * M;
+    covariance_device(filt_d, M, N, XXt, s);
+    whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
+    st.err.alloc(sizeof(int), s);
+    MS3_CUDA(cudaMemsetAsync(st.err.get(), 0, sizeof(int), s));
+    apply_whitening_device(filt_d, M, N, W, q, mixed, st.pre.ptr, s, st.err.as<int>());
+}
+}  // namespace
+
+int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream) {
+    std::string first_error;
+    int first_code = MS3GPU_OK;
+    const int rc = guarded([&] {
+        if (n_jobs < 0) throw_invalid("n_jobs is negative");
+        require(jobs, "jobs", n_jobs > 0);
+        if (n_jobs == 0) return;
+        cudaStream_t s0 = as_stream(stream);
+        const int K = std::min<int>(n_jobs, 4);
+        std::vector<cudaStream_t> streams((size_t)K, nullptr);
+        cudaEvent_t start = nullptr;
+        MS3_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+        MS3_CUDA(cudaEventRecord(start, s0));
+        for (auto& st : streams) {
+            MS3_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            MS3_CUDA(cudaStreamWaitEvent(st, start, 0));
+        }
+        std::vector<std::unique_ptr<BatchJob>> state((size_t)n_jobs);
+        auto record = [&](int i, int code, const std::string& msg) {
+            jobs[i].status = code;
+            if (code != MS3GPU_OK && first_code == MS3GPU_OK) {
+                first_code = code;
+                first_error = "job " + std::to_string(i) + ": " + msg;
+            }
+        };
+        // phase 1: every job's device work, round-robin over the streams
+        for (int i = 0; i < n_jobs; i++) {
+            state[(size_t)i].reset(new BatchJob);
+            state[(size_t)i]->s = streams[(size_t)(i % K)];
+            jobs[i].status = MS3GPU_OK;
+            const int code = guarded([&] { issue_batch_job(jobs[i], *state[(size_t)i]); });
+            if (code != MS3GPU_OK) record(i, code, ms3gpu_last_error());
+        }
+        // phase 2: copies back (a copy into pageable memory waits for its job)
+        for (int i = 0; i < n_jobs; i++) {
+            if (jobs[i].status != MS3GPU_OK) continue;
+            BatchJob& st = *state[(size_t)i];
+            const int code = guarded([&] {
+                if (jobs[i].filt_out) st.filt.finish(st.s);
+                st.pre.finish(st.s);
+            });
+            if (code != MS3GPU_OK) record(i, code, ms3gpu_last_error());
+        }
+        for (auto& st : streams) MS3_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < n_jobs; i++) {
+            if (jobs[i].status != MS3GPU_OK) continue;
+            int herr = 0;
+            const int code = guarded([&] {
+                MS3_CUDA(cudaMemcpy(&herr, state[(size_t)i]->err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+                if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+            });
+            if (code != MS3GPU_OK) record(i, code, ms3gpu_last_error());
+        }
+        state.clear();  // device buffers go back to the pools of their streams
+        for (auto& st : streams) {
+            MS3_CUDA(cudaStreamSynchronize(st));
+            MS3_CUDA(cudaStreamDestroy(st));
+        }
+        MS3_CUDA(cudaEventDestroy(start));
+        bandpass_check_timeout(s0);
+    });
+    if (rc != MS3GPU_OK) return rc;
+    if (first_code != MS3GPU_OK) {
+        g_last_error = first_error;
+        return first_code;
+    }
+    return MS3GPU_OK;
 }
 
 int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt, void* stream) {
