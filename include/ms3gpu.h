@@ -214,6 +214,18 @@ MS3GPU_API int ms3gpu_compute_whitening_matrix(const float* const* timeseries_li
                                                int32_t n_inputs, int64_t M, const int32_t* channels,
                                                int32_t n_channels, double* W_out, void* stream);
 
+/* ms3.whiten per channel block (per shank): the channels are split into
+ * n_blocks blocks -- block k holds block_sizes[k] 1-based channel numbers,
+ * listed block after block in `channels` -- that together name every channel
+ * of X exactly once.  Each block is whitened on its own (its XXt, its
+ * power-iteration W, its apply with the 1e-4 rounding) and written back to
+ * its channels of the M x N output: the same result as
+ * ms3.compute_whitening_matrix with the block's channels followed by
+ * ms3.apply_whitening_matrix on those channels. */
+MS3GPU_API int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const int32_t* channels,
+                                    const int32_t* block_sizes, int32_t n_blocks, void* timeseries_out,
+                                    const ms3gpu_whiten_opts* opts, void* stream);
+
 /* ms3.whiten_clips (p_whiten.cpp:300-345): for every timepoint of every clip
  * of an M x T x L float32 array, out(m1, t, l) = sum_m2 x(m2, t, l)
  * W[m1*M + m2] -- the apply of ms3gpu_apply_whitening_matrix without the 1e-4

@@ -91,6 +91,8 @@ SIGNATURES = {
     "ms3gpu_bandpass_whiten_batch": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_int32, _vp]),
     "ms3gpu_compute_whitening_matrix": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _i64, _vp, ctypes.c_int32, _vp,
                                                        _vp]),
+    "ms3gpu_whiten_blocks": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, ctypes.c_int32, _vp,
+                                            ctypes.POINTER(WhitenOpts), _vp]),
     "ms3gpu_whiten_clips": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
 }
 

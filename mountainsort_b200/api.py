@@ -245,6 +245,23 @@ def compute_whitening_matrix(X_list, channels=None, stream=None):
     return _mat_out(W)
 
 
+def whiten_blocks(X, blocks, quantization_unit=0.0, out=None, stream=None, precision="plain"):
+    """ms3.whiten per channel block (ms3gpu_whiten_blocks): `blocks` is a list
+    of 1-based channel-number lists that together name every channel once
+    (e.g. the shanks of a probe); each block is whitened on its own."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    ch = np.ascontiguousarray(np.concatenate([np.asarray(b, dtype=np.int32) for b in blocks]), dtype=np.int32)
+    sizes = np.ascontiguousarray([len(b) for b in blocks], dtype=np.int32)
+    if out is None:
+        out = _empty_like(X, (N, M), np.int16 if quantization_unit > 0 else np.float32)
+    o = WhitenOpts(float(quantization_unit), _PRECISION[precision])
+    check(L.ms3gpu_whiten_blocks(_ptr(X), M, N, ch.ctypes.data, sizes.ctypes.data, len(blocks), _ptr(out),
+                                 ctypes.byref(o), _stream_ptr(X, stream)))
+    return out
+
+
 def whiten_clips(clips, W, quantization_unit=0.0, out=None, stream=None, precision="plain"):
     """ms3.whiten_clips (p_whiten.cpp:300-345): clips as an (L, T, M) array
     (the .mda M x T x L layout); W^T x at every timepoint, no 1e-4 rounding;

@@ -549,6 +549,67 @@ int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const i
     });
 }
 
+int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const int32_t* channels,
+                         const int32_t* block_sizes, int32_t n_blocks, void* timeseries_out,
+                         const ms3gpu_whiten_opts* opts, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!opts) throw_invalid("whiten opts is NULL");
+        if (n_blocks < 1) throw_invalid("n_blocks must be positive");
+        require(block_sizes, "block_sizes", true);
+        require(channels, "channels", true);
+        int64_t total = 0;
+        for (int32_t k = 0; k < n_blocks; k++) {
+            if (block_sizes[k] < 1) throw_invalid("block " + std::to_string(k) + " is empty");
+            total += block_sizes[k];
+        }
+        if (total != M) throw_invalid("the blocks must name every channel exactly once");
+        std::vector<int32_t> ch0((size_t)M);
+        std::vector<char> seen((size_t)M, 0);
+        for (int64_t j = 0; j < M; j++) {
+            const int64_t c = channels[j];
+            if (c < 1 || c > M) throw_invalid("channel " + std::to_string(c) + " is outside 1.." + std::to_string(M));
+            if (seen[(size_t)(c - 1)]++) throw_invalid("channel " + std::to_string(c) + " is in two blocks");
+            ch0[(size_t)j] = (int32_t)(c - 1);
+        }
+        cudaStream_t s = as_stream(stream);
+        const double q = opts->quantization_unit;
+        const bool mixed = check_precision(opts->precision);
+        const size_t esz = q > 0 ? 2 : 4;
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(timeseries_out, "timeseries_out", M * N > 0);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(timeseries_out, esz * (size_t)(M * N), s);
+        DevBuf chmap(sizeof(int32_t) * (size_t)M, s);
+        MS3_CUDA(cudaMemcpyAsync(chmap.get(), ch0.data(), sizeof(int32_t) * (size_t)M, cudaMemcpyHostToDevice, s));
+        DevBuf err(sizeof(int), s);
+        MS3_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), s));
+        int64_t off = 0;
+        for (int32_t k = 0; k < n_blocks; k++) {
+            const int64_t Mb = block_sizes[k];
+            const int32_t* chk = chmap.as<int32_t>() + off;
+            DevBuf xb(sizeof(float) * (size_t)(Mb * N), s), yb(esz * (size_t)(Mb * N), s);
+            DevBuf mats(sizeof(double) * (size_t)(2 * Mb * Mb), s);
+            gather_channels_device(static_cast<const float*>(in.ptr), M, N, chk, Mb, xb.as<float>(), s);
+            double* XXt = mats.as<double>();
+            double* W = XXt + Mb * Mb;
+            covariance_device(xb.as<float>(), Mb, N, XXt, s);
+            whitening_matrix_device(XXt, Mb, W, nullptr, nullptr, s);
+            apply_whitening_device(xb.as<float>(), Mb, N, W, q, mixed, yb.get(), s, err.as<int>());
+            scatter_channels_device(yb.get(), Mb, N, chk, M, out.ptr, esz, s);
+            off += Mb;
+        }
+        out.finish(s);
+        int herr = 0;
+        MS3_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        MS3_CUDA(cudaStreamSynchronize(s));
+        if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+    });
+}
+
 int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* W,
                         double quantization_unit, int32_t precision, void* clips_out, void* stream) {
     return guarded([&] {

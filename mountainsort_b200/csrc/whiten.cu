@@ -480,6 +480,18 @@ __global__ void gather_channels(const float* __restrict__ X, int64_t M, int64_t 
     }
 }
 
+// out[t][ch[j]] = Y[t][j]: a whitened channel block back into its columns
+// (element size 4 for float32 output, 2 for int16).
+template <class T>
+__global__ void scatter_channels(const T* __restrict__ Y, int64_t M2, int64_t N, const int32_t* __restrict__ ch,
+                                 int64_t M, T* __restrict__ out) {
+    const int64_t total = N * M2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = i / M2, j = i - t * M2;
+        out[t * M + ch[j]] = Y[i];
+    }
+}
+
 int num_sms() {
     int dev = 0, n = 0;
     MS3_CUDA(cudaGetDevice(&dev));
@@ -665,6 +677,19 @@ void gather_channels_device(const float* X, int64_t M, int64_t N, const int32_t*
     if (N <= 0 || M2 <= 0) return;
     const int64_t blocks = std::min<int64_t>(ceil_div(N * M2, 256), (int64_t)num_sms() * 32);
     gather_channels<<<(unsigned)blocks, 256, 0, stream>>>(X, M, N, ch, M2, out);
+    MS3_LAUNCH_CHECK();
+}
+
+void scatter_channels_device(const void* Y, int64_t M2, int64_t N, const int32_t* ch, int64_t M, void* out,
+                             size_t elem, cudaStream_t stream) {
+    if (N <= 0 || M2 <= 0) return;
+    const int64_t blocks = std::min<int64_t>(ceil_div(N * M2, 256), (int64_t)num_sms() * 32);
+    if (elem == 2)
+        scatter_channels<int16_t><<<(unsigned)blocks, 256, 0, stream>>>(static_cast<const int16_t*>(Y), M2, N, ch, M,
+                                                                        static_cast<int16_t*>(out));
+    else
+        scatter_channels<float><<<(unsigned)blocks, 256, 0, stream>>>(static_cast<const float*>(Y), M2, N, ch, M,
+                                                                      static_cast<float*>(out));
     MS3_LAUNCH_CHECK();
 }
 

@@ -34,6 +34,10 @@ int64_t covariance_noalloc_max_channels();
 void gather_channels_device(const float* X, int64_t M, int64_t N, const int32_t* ch, int64_t M2, float* out,
                             cudaStream_t stream);
 
+// out (N x M rows) columns ch[j] = Y (N x M2 rows) column j; elem 4 (float32) or 2 (int16).
+void scatter_channels_device(const void* Y, int64_t M2, int64_t N, const int32_t* ch, int64_t M, void* out,
+                             size_t elem, cudaStream_t stream);
+
 // Power-iteration whitening matrix; comps / sigma may be null.
 void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
                              cudaStream_t stream);
