@@ -233,6 +233,18 @@ MS3GPU_API int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t 
 MS3GPU_API int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* W,
                                    double quantization_unit, int32_t precision, void* clips_out, void* stream);
 
+/* ms3.mask_out_artifacts (p_mask_out_artifacts.cpp:24-104): per channel the
+ * norm of every whole interval of interval_size timepoints; an interval
+ * whose norm exceeds the channel's mean + threshold * stdev (over its
+ * intervals) is zeroed together with its two neighbours, on all channels;
+ * timepoints after the last whole interval are zero.  float32 M x N in and
+ * out.  threshold == 0 or interval_size <= 0 is MS3GPU_ERR_INVALID (the
+ * reference refuses them).  *timepoints_kept (may be NULL) receives the
+ * number of timepoints kept. */
+MS3GPU_API int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int64_t N, double threshold,
+                                         int64_t interval_size, float* timeseries_out, int64_t* timepoints_kept,
+                                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

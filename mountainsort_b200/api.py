@@ -262,6 +262,22 @@ def whiten_blocks(X, blocks, quantization_unit=0.0, out=None, stream=None, preci
     return out
 
 
+def mask_out_artifacts(X, threshold=6.0, interval_size=2000, out=None, stream=None, return_kept=False):
+    """ms3.mask_out_artifacts (p_mask_out_artifacts.cpp:24-104) on an (N, M)
+    array: intervals whose norm is an outlier on any channel are zeroed with
+    their neighbours.  Returns the masked array (and the number of
+    timepoints kept when return_kept)."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    if out is None:
+        out = _empty_like(X, (N, M), np.float32)
+    kept = ctypes.c_int64()
+    check(L.ms3gpu_mask_out_artifacts(_ptr(X), M, N, float(threshold), int(interval_size), _ptr(out),
+                                      ctypes.addressof(kept), _stream_ptr(X, stream)))
+    return (out, kept.value) if return_kept else out
+
+
 def whiten_clips(clips, W, quantization_unit=0.0, out=None, stream=None, precision="plain"):
     """ms3.whiten_clips (p_whiten.cpp:300-345): clips as an (L, T, M) array
     (the .mda M x T x L layout); W^T x at every timepoint, no 1e-4 rounding;

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "artifacts.h"
 #include "bandpass.h"
 #include "common.cuh"
 #include "ms3gpu.h"
@@ -607,6 +608,30 @@ int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const in
         MS3_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         MS3_CUDA(cudaStreamSynchronize(s));
         if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+    });
+}
+
+int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int64_t N, double threshold,
+                              int64_t interval_size, float* timeseries_out, int64_t* timepoints_kept,
+                              void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        // p_mask_out_artifacts.cpp:26-29
+        if (threshold == 0 || interval_size <= 0)
+            throw_invalid("Problem with input parameters. Either threshold or interval_size is zero.");
+        cudaStream_t s = as_stream(stream);
+        const size_t bytes = sizeof(float) * (size_t)(M * N);
+        require(timeseries, "timeseries", bytes > 0);
+        require(timeseries_out, "timeseries_out", bytes > 0);
+        InView in;
+        stage_in(in, timeseries, bytes, s);
+        OutView out;
+        out.setup(timeseries_out, bytes, s);
+        const int64_t kept = mask_out_artifacts_device(static_cast<const float*>(in.ptr), M, N, threshold,
+                                                       interval_size, static_cast<float*>(out.ptr), s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+        if (timepoints_kept) *timepoints_kept = kept;
     });
 }
 

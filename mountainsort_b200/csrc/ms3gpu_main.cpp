@@ -1,6 +1,7 @@
 // ms3gpu.mp -- MountainLab processor executable for ms3.bandpass_filter,
-// ms3.whiten, ms3.compute_whitening_matrix, ms3.apply_whitening_matrix and
-// ms3.whiten_clips, backed by libms3gpu (CUDA, sm_100a).
+// ms3.whiten, ms3.compute_whitening_matrix, ms3.apply_whitening_matrix,
+// ms3.whiten_clips and ms3.mask_out_artifacts, backed by libms3gpu (CUDA,
+// sm_100a).
 //
 // Same command-line protocol as the reference's ms3.mp
 // (packages/ms3/mountainsort3_main.cpp:379-821):
@@ -163,6 +164,11 @@ std::string spec_compute_whitening_matrix(const std::string& ind) {
 std::string spec_whiten_clips(const std::string& ind) {
     return processor_spec("ms3.whiten_clips", "0.1", {"clips", "whitening_matrix"}, {"clips_out"},
                           {{"quantization_unit", true, "0"}}, ind, false);
+}
+// mountainsort3_main.cpp:343-350
+std::string spec_mask_out_artifacts(const std::string& ind) {
+    return processor_spec("ms3.mask_out_artifacts", "0.1", {"timeseries"}, {"timeseries_out"},
+                          {{"threshold", true, "6"}, {"interval_size", true, "2000"}}, ind, false);
 }
 std::string spec_apply_whitening_matrix(const std::string& ind) {
     return processor_spec("ms3.apply_whitening_matrix", "0.1", {"timeseries", "whitening_matrix"},
@@ -377,6 +383,31 @@ int run_whiten_clips(const CLParams& clp) {
     return 0;
 }
 
+// p_mask_out_artifacts (p_mask_out_artifacts.cpp:24-104) with the arguments
+// of mountainsort3_main.cpp:782-787 (interval_size read as a double, then
+// truncated to an integer)
+int run_mask_out_artifacts(const CLParams& clp) {
+    const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
+    const double threshold = clp.num("threshold", 0);
+    const int64_t interval_size = (int64_t)clp.num("interval_size", 0);
+    if (!threshold || !interval_size) {
+        std::printf("Problem with input parameters. Either threshold or interval_size is zero.\n");
+        return -1;
+    }
+    std::string err;
+    std::vector<float> X;
+    int64_t M = 0, N = 0;
+    if (!ms3io::read_timeseries_any_f32(in, M, N, X, err)) return fail(err);
+    std::vector<float> Y((size_t)(M * N));
+    int64_t kept = 0;
+    if (ms3gpu_mask_out_artifacts(X.data(), M, N, threshold, interval_size, Y.data(), &kept, nullptr) != MS3GPU_OK)
+        return fail(ms3gpu_last_error());
+    if (!ms3io::write_timeseries(out, ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    const int64_t nint = N / interval_size;
+    if (nint > 0) std::printf("Using %.2f%% of all timepoints\n", kept * 100.0 / (double)(nint * interval_size));
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -387,16 +418,17 @@ int main(int argc, char** argv) {
     if (arg1 == "spec") {
         std::string (*const specs[])(const std::string&) = {spec_bandpass, spec_whiten,
                                                              spec_compute_whitening_matrix, spec_whiten_clips,
-                                                             spec_apply_whitening_matrix};
+                                                             spec_apply_whitening_matrix, spec_mask_out_artifacts};
         const char* const names[] = {"ms3.bandpass_filter", "ms3.whiten", "ms3.compute_whitening_matrix",
-                                     "ms3.whiten_clips", "ms3.apply_whitening_matrix"};
+                                     "ms3.whiten_clips", "ms3.apply_whitening_matrix", "ms3.mask_out_artifacts"};
+        const size_t nspec = sizeof(names) / sizeof(names[0]);
         if (arg2.empty()) {
             std::string all;
-            for (size_t i = 0; i < 5; i++) all += (i ? ",\n" : "") + specs[i]("        ");
+            for (size_t i = 0; i < nspec; i++) all += (i ? ",\n" : "") + specs[i]("        ");
             std::printf("{\n    \"processors\": [\n%s\n    ]\n}\n\n", all.c_str());
             return 0;
         }
-        for (size_t i = 0; i < 5; i++) {
+        for (size_t i = 0; i < nspec; i++) {
             if (arg2 == names[i]) {
                 std::printf("%s\n\n", specs[i]("").c_str());
                 return 0;
@@ -417,6 +449,7 @@ int main(int argc, char** argv) {
         if (pname == "ms3.compute_whitening_matrix") return run_compute_whitening_matrix(clp);
         if (pname == "ms3.apply_whitening_matrix") return run_apply_whitening_matrix(clp);
         if (pname == "ms3.whiten_clips") return run_whiten_clips(clp);
+        if (pname == "ms3.mask_out_artifacts") return run_mask_out_artifacts(clp);
     }
     std::fprintf(stderr, "Unexpected processor name: %s\n", pname.c_str());
     return -1;

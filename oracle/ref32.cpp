@@ -478,6 +478,57 @@ void ref32_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, con
     }
 }
 
+// ms3.mask_out_artifacts (packages/ms3/p_mask_out_artifacts.cpp:24-104) on
+// an M x N column-major float32 timeseries: interval norms in double (the
+// reader delivers doubles), MLCompute::mean / stdev (common/mlcompute.cpp:
+// 67-85), flagged intervals masked with their neighbours (the reference's
+// write to use_it[-1] for interval 0 is out of bounds and dropped here),
+// output zero on masked intervals and after the last whole interval.
+// Returns the number of timepoints kept, or -1 for a zero threshold or
+// interval size (the reference returns false).
+int64_t ref32_mask_out_artifacts(const float* X, int64_t M, int64_t N, double threshold, int64_t interval_size,
+                                 float* out) {
+    if (!threshold || !interval_size) return -1;
+    const int64_t I = interval_size, nint = N / I;
+    std::vector<double> norms((size_t)(M * nint));
+    for (int64_t i = 0; i < nint; i++) {
+        for (int64_t m = 0; m < M; m++) {
+            double sumsqr = 0;
+            for (int64_t aa = 0; aa < I; aa++) {
+                const double v = X[(i * I + aa) * M + m];
+                sumsqr += v * v;
+            }
+            norms[(size_t)(m + M * i)] = std::sqrt(sumsqr);
+        }
+    }
+    std::vector<int> use_it((size_t)(nint + 1), 1);
+    for (int64_t m = 0; m < M; m++) {
+        double sum = 0, sumsqr = 0;
+        for (int64_t i = 0; i < nint; i++) {
+            const double v = norms[(size_t)(m + M * i)];
+            sum = sum + v;
+            sumsqr = sumsqr + v * v;
+        }
+        const double mean0 = nint ? sum / nint : 0;
+        const double sigma0 = nint >= 2 ? std::sqrt((sumsqr - sum * sum / nint) / (nint - 1)) : 0;
+        for (int64_t i = 0; i < nint; i++) {
+            if (norms[(size_t)(m + M * i)] > mean0 + sigma0 * threshold) {
+                if (i >= 1) use_it[(size_t)(i - 1)] = 0;
+                use_it[(size_t)i] = 0;
+                use_it[(size_t)(i + 1)] = 0;
+            }
+        }
+    }
+    std::fill(out, out + M * N, 0.f);
+    int64_t kept = 0;
+    for (int64_t i = 0; i < nint; i++) {
+        if (!use_it[(size_t)i]) continue;
+        kept += I;
+        std::memcpy(out + i * I * M, X + i * I * M, sizeof(float) * (size_t)(I * M));
+    }
+    return kept;
+}
+
 // Whole ms3.whiten on an in-memory timeseries.  Also returns XXt and W when
 // the caller passes buffers for them.
 int ref32_whiten(const float* X, int64_t M, int64_t N, double quantization_unit, int exec_threads,

@@ -56,6 +56,8 @@ def lib():
                                                      ctypes.POINTER(ctypes.c_int32), c_int, _dp, _dp]
         L.ref32_compute_whitening_matrix.restype = c_int
         L.ref32_whiten_clips.argtypes = [_fp, c_i64, c_i64, c_i64, _dp, c_dbl, _fp]
+        L.ref32_mask_out_artifacts.argtypes = [_fp, c_i64, c_i64, c_dbl, c_i64, _fp]
+        L.ref32_mask_out_artifacts.restype = c_i64
         L.ref32_float_to_int16.argtypes = [ctypes.c_float]
         L.ref32_float_to_int16.restype = ctypes.c_int16
         _lib = L
@@ -185,3 +187,14 @@ def whiten_clips(clips, W, quantization_unit=0.0):
     if quantization_unit > 0:
         return float_to_int16(out)
     return out
+
+
+def mask_out_artifacts(X_rows, threshold=6.0, interval_size=2000):
+    """ms3.mask_out_artifacts on an (N, M) float32 array; returns (out, kept)."""
+    X = np.ascontiguousarray(X_rows, dtype=np.float32)
+    N, M = X.shape
+    out = np.zeros_like(X)
+    kept = lib().ref32_mask_out_artifacts(_f(X), M, N, float(threshold), int(interval_size), _f(out))
+    if kept < 0:
+        raise ValueError("Problem with input parameters. Either threshold or interval_size is zero.")
+    return out, kept

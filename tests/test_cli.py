@@ -25,7 +25,7 @@ def test_spec_lists_the_processors():
     spec = json.loads(r.stdout)
     by = {p["name"]: p for p in spec["processors"]}
     assert set(by) == {"ms3.bandpass_filter", "ms3.whiten", "ms3.compute_whitening_matrix",
-                       "ms3.whiten_clips", "ms3.apply_whitening_matrix"}
+                       "ms3.whiten_clips", "ms3.apply_whitening_matrix", "ms3.mask_out_artifacts"}
     bp = by["ms3.bandpass_filter"]
     assert bp["version"] == "0.20"
     params = {p["name"]: p for p in bp["parameters"]}
@@ -148,3 +148,16 @@ def test_directory_input_is_concatenated_like_diskreadmda32(tmp_path, ref32):
     r = run("ms3.bandpass_filter", f"--timeseries={d}", f"--timeseries_out={out}", "--samplerate=30000",
             "--freq_min=300", "--freq_max=0")
     assert r.returncode == 255 and not os.path.exists(out)
+
+
+def test_mask_out_artifacts_spec_and_parameter_check(tmp_path):
+    # mountainsort3_main.cpp:343-350; zero threshold / interval refused (p_mask_out_artifacts.cpp:26-29)
+    ma = {p["name"]: p for p in json.loads(run("spec").stdout)["processors"]}["ms3.mask_out_artifacts"]
+    assert ma["version"] == "0.1" and "requirements_command" not in ma
+    params = {p["name"]: p for p in ma["parameters"]}
+    assert params["threshold"]["default_value"] == 6 and params["interval_size"]["default_value"] == 2000
+    p = str(tmp_path / "x.mda")
+    mdaio.writemda(np.zeros((4, 100), np.float32), p)
+    out = str(tmp_path / "o.mda")
+    r = run("ms3.mask_out_artifacts", f"--timeseries={p}", f"--timeseries_out={out}", "--threshold=0")
+    assert r.returncode == 255 and "zero" in r.stdout and not os.path.exists(out)

@@ -229,3 +229,30 @@ def test_whiten_clips_oracle_has_no_1e4_rounding(ref32):
     out16 = ref32.whiten_clips(clips, W, quantization_unit=q)
     assert out16.dtype == np.int16
     assert np.abs(out16.astype(np.float64) - np.trunc(out.astype(np.float64) / q + 0.5)).max() <= 1
+
+
+def test_mask_out_artifacts_oracle(ref32):
+    # p_mask_out_artifacts.cpp:24-104 restated in numpy
+    rng = np.random.default_rng(2)
+    M, I, nint = 6, 100, 40
+    N = nint * I + 37  # a tail beyond the last whole interval
+    X = rng.standard_normal((N, M)).astype(np.float32)
+    X[5 * I + 10, 2] = 80.0  # artifact in interval 5
+    X[3, 4] = 80.0  # artifact in interval 0 (the reference also writes use_it[-1])
+    out, kept = ref32.mask_out_artifacts(X, threshold=6, interval_size=I)
+    norms = np.sqrt((X[: nint * I].astype(np.float64) ** 2).reshape(nint, I, M).sum(axis=1))
+    use = np.ones(nint + 1, bool)
+    for m in range(M):
+        v = norms[:, m]
+        lim = v.mean() + v.std(ddof=1) * 6
+        for i in np.nonzero(v > lim)[0]:
+            use[max(i - 1, 0):i + 2] = False
+    assert not use[0] and not use[1] and not use[4] and not use[5] and not use[6] and use[2] and use[7]
+    expect = np.zeros_like(X)
+    for i in range(nint):
+        if use[i]:
+            expect[i * I:(i + 1) * I] = X[i * I:(i + 1) * I]
+    np.testing.assert_array_equal(out, expect)
+    assert kept == use[:nint].sum() * I
+    with pytest.raises(ValueError):
+        ref32.mask_out_artifacts(X, threshold=0)
