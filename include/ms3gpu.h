@@ -245,6 +245,29 @@ MS3GPU_API int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int
                                          int64_t interval_size, float* timeseries_out, int64_t* timepoints_kept,
                                          void* stream);
 
+/* Event detection of mountainsortalg on a (whitened) timeseries, the first
+ * consumer of this path's output: detect_events
+ * (mountainsortalg/detect_events.cpp:69-135) as NeighborhoodSorter::
+ * addTimeChunk applies it (neighborhoodsorter.cpp:74-100) to every channel
+ * (each channel is the centre of its own neighborhood) over the time chunks
+ * of p_mountainsort3.cpp:190-215: chunks of chunk_size timepoints with 1000
+ * timepoints of padding on both sides (zeros outside the recording), the
+ * chunk's mean and stdev, samples whose deviation (sign > 0), negated
+ * deviation (sign < 0) or absolute deviation (sign == 0) exceeds
+ * detect_threshold * stdev, the greedy strongest-within-detect_interval rule,
+ * times kept inside the unpadded chunk.  chunk_size <= 0 selects the
+ * reference's get_time_chunk_infos length for one simultaneous batch
+ * (p_mountainsort3.cpp:507-517).
+ *
+ * counts (M entries) receives each channel's number of events; times
+ * receives all events, channel after channel, each channel's times sorted
+ * (timepoint indices).  times may be NULL to ask for counts only; when the
+ * events exceed `capacity` the call fails with MS3GPU_ERR_INVALID after
+ * filling counts. */
+MS3GPU_API int ms3gpu_detect_events(const float* timeseries, int64_t M, int64_t N, double detect_threshold,
+                                    double detect_interval, int32_t detect_sign, int64_t chunk_size, int64_t* counts,
+                                    int64_t* times, int64_t capacity, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,7 @@ SIGNATURES = {
     "ms3gpu_whiten_blocks": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, ctypes.c_int32, _vp,
                                             ctypes.POINTER(WhitenOpts), _vp]),
     "ms3gpu_mask_out_artifacts": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _i64, _vp, _vp, _vp]),
+    "ms3gpu_detect_events": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _dbl, ctypes.c_int32, _i64, _vp, _vp, _i64, _vp]),
     "ms3gpu_whiten_clips": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
 }
 

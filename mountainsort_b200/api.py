@@ -278,6 +278,27 @@ def mask_out_artifacts(X, threshold=6.0, interval_size=2000, out=None, stream=No
     return (out, kept.value) if return_kept else out
 
 
+def detect_events(X, detect_threshold=3.0, detect_interval=10.0, detect_sign=0, chunk_size=0, stream=None):
+    """Event detection of mountainsortalg (detect_events.cpp:69-135 over the
+    time chunks of p_mountainsort3.cpp:190-215) for every channel of an
+    (N, M) array.  Returns a list of M int64 arrays of event timepoints."""
+    L = _lib.load()
+    X = _as_f32_rows(X)
+    N, M = X.shape
+    counts = np.zeros(max(M, 1), np.int64)
+    args = (_ptr(X), M, N, float(detect_threshold), float(detect_interval), int(detect_sign), int(chunk_size))
+    # room for 1% of the samples as events; a second call only when that is too little
+    cap = max(1024, (N * M) // 100)
+    times = np.empty(cap, np.int64)
+    rc = L.ms3gpu_detect_events(*args, counts.ctypes.data, times.ctypes.data, cap, _stream_ptr(X, stream))
+    total = int(counts[:M].sum())
+    if rc == _lib.ERR_INVALID and total > cap:
+        times = np.empty(total, np.int64)
+        rc = L.ms3gpu_detect_events(*args, counts.ctypes.data, times.ctypes.data, total, _stream_ptr(X, stream))
+    check(rc)
+    return np.split(times[:total], np.cumsum(counts[:M])[:-1]) if M else []
+
+
 def whiten_clips(clips, W, quantization_unit=0.0, out=None, stream=None, precision="plain"):
     """ms3.whiten_clips (p_whiten.cpp:300-345): clips as an (L, T, M) array
     (the .mda M x T x L layout); W^T x at every timepoint, no 1e-4 rounding;

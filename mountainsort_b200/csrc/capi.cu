@@ -7,6 +7,7 @@
 // codes plus the per-thread text returned by ms3gpu_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "artifacts.h"
 #include "bandpass.h"
+#include "detect.h"
 #include "common.cuh"
 #include "ms3gpu.h"
 #include "pipeline.h"
@@ -632,6 +634,30 @@ int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int64_t N, dou
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
         if (timepoints_kept) *timepoints_kept = kept;
+    });
+}
+
+int ms3gpu_detect_events(const float* timeseries, int64_t M, int64_t N, double detect_threshold,
+                         double detect_interval, int32_t detect_sign, int64_t chunk_size, int64_t* counts,
+                         int64_t* times, int64_t capacity, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        require(counts, "counts", M > 0);
+        cudaStream_t s = as_stream(stream);
+        const size_t bytes = sizeof(float) * (size_t)(M * N);
+        require(timeseries, "timeseries", bytes > 0);
+        const int64_t chunk = chunk_size > 0 ? chunk_size : detect_chunk_size(M, N, 1);
+        InView in;
+        stage_in(in, timeseries, bytes, s);
+        std::vector<int64_t> c, t;
+        detect_events_device(static_cast<const float*>(in.ptr), M, N, detect_threshold, detect_interval, detect_sign,
+                             chunk, 1000, c, t, s);
+        for (int64_t m = 0; m < M; m++) counts[m] = c[(size_t)m];
+        if (!times) return;
+        if ((int64_t)t.size() > capacity)
+            throw_invalid("times needs " + std::to_string(t.size()) + " entries (capacity " +
+                          std::to_string(capacity) + ")");
+        std::copy(t.begin(), t.end(), times);
     });
 }
 

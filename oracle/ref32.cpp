@@ -529,6 +529,93 @@ int64_t ref32_mask_out_artifacts(const float* X, int64_t M, int64_t N, double th
     return kept;
 }
 
+// mountainsortalg's detect_events (detect_events.cpp:69-135) on one vector.
+static std::vector<int64_t> detect_events_vec(const std::vector<double>& X, double detect_threshold,
+                                              double detect_interval, int sign) {
+    const int64_t ct = (int64_t)X.size();
+    double sum = 0, sumsqr = 0;
+    for (double v : X) sum = sum + v;
+    for (double v : X) sumsqr = sumsqr + v * v;
+    const double mean = ct ? sum / ct : 0;
+    const double stdev = ct >= 2 ? std::sqrt((sumsqr - sum * sum / ct) / (ct - 1)) : 0;
+    const double threshold2 = detect_threshold * stdev;
+    std::vector<int64_t> tc;
+    std::vector<double> vc;
+    for (int64_t n = 0; n < ct; n++) {
+        double val = X[(size_t)n] - mean;
+        if (sign < 0)
+            val = -val;
+        else if (sign == 0)
+            val = std::fabs(val);
+        if (val > threshold2) {
+            tc.push_back(n);
+            vc.push_back(val);
+        }
+    }
+    std::vector<char> to_use(tc.size(), 0);
+    int64_t last_best_ind = -1;
+    for (int64_t i = 0; i < (int64_t)tc.size(); i++) {
+        if (last_best_ind >= 0) {
+            if (tc[(size_t)last_best_ind] < tc[(size_t)i] - detect_interval) {
+                last_best_ind = -1;
+                if ((i > 0) && (tc[(size_t)i - 1] >= tc[(size_t)i] - detect_interval)) {
+                    last_best_ind = i - 1;
+                    int64_t jj = last_best_ind;
+                    while ((jj - 1 >= 0) && (tc[(size_t)jj - 1] >= tc[(size_t)i] - detect_interval)) {
+                        if (vc[(size_t)jj - 1] > vc[(size_t)last_best_ind]) last_best_ind = jj - 1;
+                        jj--;
+                    }
+                }
+            }
+        }
+        if (last_best_ind >= 0) {
+            if (vc[(size_t)i] > vc[(size_t)last_best_ind]) {
+                to_use[(size_t)i] = 1;
+                to_use[(size_t)last_best_ind] = 0;
+                last_best_ind = i;
+            } else {
+                to_use[(size_t)i] = 0;
+            }
+        } else {
+            to_use[(size_t)i] = 1;
+            last_best_ind = i;
+        }
+    }
+    std::vector<int64_t> times;
+    for (size_t i = 0; i < tc.size(); i++)
+        if (to_use[i]) times.push_back(tc[i]);
+    return times;
+}
+
+// detect_events on every channel over mountainsort3's time chunks (chunk
+// timepoints, `pad` of padding each side, zeros outside [0, N); times kept
+// inside the unpadded chunk, neighborhoodsorter.cpp:74-100).  counts[m] and
+// times channel after channel; returns the total (times written up to
+// capacity).
+int64_t ref32_detect_events(const float* X, int64_t M, int64_t N, double detect_threshold, double detect_interval,
+                            int sign, int64_t chunk, int64_t pad, int64_t* counts, int64_t* times, int64_t capacity) {
+    int64_t total = 0;
+    for (int64_t m = 0; m < M; m++) {
+        counts[m] = 0;
+        for (int64_t t1 = 0; t1 < N; t1 += chunk) {
+            const int64_t size = std::min(chunk, N - t1);
+            std::vector<double> X0((size_t)(size + 2 * pad));
+            for (int64_t n = 0; n < size + 2 * pad; n++) {
+                const int64_t t = t1 - pad + n;
+                X0[(size_t)n] = (t >= 0 && t < N) ? (double)X[t * M + m] : 0.0;
+            }
+            for (int64_t t0 : detect_events_vec(X0, detect_threshold, detect_interval, sign)) {
+                if ((0 <= t0 - pad) && (t0 - pad < size)) {
+                    if (total < capacity) times[total] = t0 - pad + t1;
+                    total++;
+                    counts[m]++;
+                }
+            }
+        }
+    }
+    return total;
+}
+
 // Whole ms3.whiten on an in-memory timeseries.  Also returns XXt and W when
 // the caller passes buffers for them.
 int ref32_whiten(const float* X, int64_t M, int64_t N, double quantization_unit, int exec_threads,

@@ -58,6 +58,9 @@ def lib():
         L.ref32_whiten_clips.argtypes = [_fp, c_i64, c_i64, c_i64, _dp, c_dbl, _fp]
         L.ref32_mask_out_artifacts.argtypes = [_fp, c_i64, c_i64, c_dbl, c_i64, _fp]
         L.ref32_mask_out_artifacts.restype = c_i64
+        L.ref32_detect_events.argtypes = [_fp, c_i64, c_i64, c_dbl, c_dbl, c_int, c_i64, c_i64,
+                                          ctypes.POINTER(c_i64), ctypes.POINTER(c_i64), c_i64]
+        L.ref32_detect_events.restype = c_i64
         L.ref32_float_to_int16.argtypes = [ctypes.c_float]
         L.ref32_float_to_int16.restype = ctypes.c_int16
         _lib = L
@@ -198,3 +201,20 @@ def mask_out_artifacts(X_rows, threshold=6.0, interval_size=2000):
     if kept < 0:
         raise ValueError("Problem with input parameters. Either threshold or interval_size is zero.")
     return out, kept
+
+
+def detect_events(X_rows, detect_threshold=3.0, detect_interval=10.0, detect_sign=0, chunk_size=None, pad=1000):
+    """mountainsortalg's event detection on every channel over mountainsort3's
+    time chunks; returns a list of per-channel int64 time arrays."""
+    X = np.ascontiguousarray(X_rows, dtype=np.float32)
+    N, M = X.shape
+    if not chunk_size:
+        chunk_size = max(20000, min(N, int(1e9) // (M * 4)))
+    counts = np.zeros(M, np.int64)
+    cap = N * M // 2 + 1
+    times = np.zeros(cap, np.int64)
+    p64 = ctypes.POINTER(c_i64)
+    total = lib().ref32_detect_events(_f(X), M, N, float(detect_threshold), float(detect_interval), int(detect_sign),
+                                      int(chunk_size), int(pad), counts.ctypes.data_as(p64),
+                                      times.ctypes.data_as(p64), cap)
+    return np.split(times[:total], np.cumsum(counts)[:-1])

@@ -256,3 +256,19 @@ def test_mask_out_artifacts_oracle(ref32):
     assert kept == use[:nint].sum() * I
     with pytest.raises(ValueError):
         ref32.mask_out_artifacts(X, threshold=0)
+
+
+def test_detect_events_oracle_on_planted_spikes(ref32):
+    # detect_events.cpp:69-135: above threshold*stdev, strongest within detect_interval
+    rng = np.random.default_rng(4)
+    N, M = 60000, 3
+    X = rng.standard_normal((N, M)).astype(np.float32)
+    X[1000, 0] = -30.0                   # isolated negative spike
+    X[5000, 0], X[5006, 0] = 20.0, 25.0  # two within 10 samples: the stronger wins
+    X[9000, 1] = 40.0
+    times = ref32.detect_events(X, detect_threshold=8, detect_interval=10, detect_sign=0, chunk_size=20000)
+    assert list(times[0]) == [1000, 5006] and list(times[1]) == [9000] and len(times[2]) == 0
+    neg = ref32.detect_events(X, detect_threshold=8, detect_interval=10, detect_sign=-1, chunk_size=20000)
+    assert list(neg[0]) == [1000]
+    pos = ref32.detect_events(X, detect_threshold=8, detect_interval=10, detect_sign=1, chunk_size=20000)
+    assert list(pos[0]) == [5006] and list(pos[1]) == [9000]
