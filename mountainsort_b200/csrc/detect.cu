@@ -44,11 +44,18 @@ __device__ __forceinline__ float sample(const float* X, int64_t M, int64_t N, in
 
 // kBatch consecutive samples of channel m from timepoint t, loaded together so
 // that their latencies overlap (zeros outside [0, N) and beyond `left`).
-constexpr int kBatch = 64;
+constexpr int kBatch = 32;
 __device__ __forceinline__ void load_batch(const float* X, int64_t M, int64_t N, int64_t t, int64_t m, int64_t left,
                                            float (&b)[kBatch]) {
+    if (t >= 0 && t + kBatch <= N && left >= kBatch) {
+        // interior: unconditional loads, all in flight together
+        const float* p = X + t * M + m;
 #pragma unroll
-    for (int k = 0; k < kBatch; k++) b[k] = (k < left) ? sample(X, M, N, t + k, m) : 0.f;
+        for (int k = 0; k < kBatch; k++) b[k] = __ldg(p + (int64_t)k * M);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) b[k] = (k < left) ? sample(X, M, N, t + k, m) : 0.f;
+    }
 }
 
 __device__ __forceinline__ int64_t chunk_size_at(int64_t c, int64_t chunk, int64_t N) {
