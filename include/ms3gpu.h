@@ -47,6 +47,7 @@ extern "C" {
 #define MS3GPU_ERR_CUDA -2        /* a CUDA runtime error */
 #define MS3GPU_ERR_UNSUPPORTED -3 /* a shape the GPU path does not handle */
 #define MS3GPU_ERR_NOMEM -4       /* device memory exhausted */
+#define MS3GPU_ERR_IO -5          /* a read or write callback of a streaming call failed */
 
 /* .mda data type codes (packages/ms3/mda/mdaio.h:55-62) used for outputs. */
 #define MS3GPU_DTYPE_FLOAT32 -3
@@ -267,6 +268,55 @@ MS3GPU_API int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int
 MS3GPU_API int ms3gpu_detect_events(const float* timeseries, int64_t M, int64_t N, double detect_threshold,
                                     double detect_interval, int32_t detect_sign, int64_t chunk_size, int64_t* counts,
                                     int64_t* times, int64_t capacity, void* stream);
+
+/* Streaming I/O.  The reference never holds a recording in memory: its
+ * processors read chunks through DiskReadMda32::readChunk
+ * (mda/diskreadmda32.cpp:615-661) and write them through
+ * DiskWriteMda::writeChunk (mda/diskwritemda.cpp:255-265).  The streaming
+ * entry points take the same shape of access as callbacks:
+ *
+ *   read(read_ctx, t0, nt, dst): fill dst with timepoints [t0, t0 + nt) of
+ *     the input, M values per timepoint (channel fastest), in the input
+ *     dtype; 0 <= t0 and t0 + nt <= N.
+ *   write(write_ctx, t0, nt, src): take output timepoints [t0, t0 + nt),
+ *     M values per timepoint, in the output dtype.
+ *
+ * Both return 0 on success; anything else stops the call with MS3GPU_ERR_IO.
+ * They are called from the calling thread, in increasing t0, and each
+ * buffer is valid only during its call.  Output timepoints that no write
+ * covers (the gaps between subsampled chunks) are zero, as in the reference's
+ * preallocated file.  slab_bytes bounds the rows of one read (about that
+ * many bytes; 0 = 1 GiB); the call holds two slabs of input and two of
+ * output in pinned host memory and as many on the device. */
+typedef int (*ms3gpu_read_fn)(void* ctx, int64_t t0, int64_t nt, void* dst);
+typedef int (*ms3gpu_write_fn)(void* ctx, int64_t t0, int64_t nt, const void* src);
+
+typedef struct ms3gpu_stream_io {
+    ms3gpu_read_fn read;
+    void* read_ctx;
+    ms3gpu_write_fn write;
+    void* write_ctx;
+    int64_t slab_bytes;
+} ms3gpu_stream_io;
+
+/* ms3.bandpass_filter over a recording of M x N read and written through
+ * `io`: the processor's own chunk loop (p_bandpass_filter.cpp:160-220).
+ * in_dtype: MS3GPU_DTYPE_FLOAT32 or MS3GPU_DTYPE_INT16 (converted on load as
+ * ms3gpu_bandpass_filter_i16 does).  The output has the shape and dtype of
+ * ms3gpu_bandpass_output_dims(), except that freq_max == 0 copies the input
+ * rows unchanged in in_dtype.  Every output value equals the in-memory call's. */
+MS3GPU_API int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dtype, const ms3gpu_stream_io* io,
+                                             const ms3gpu_bandpass_opts* opts, void* stream);
+
+/* ms3.whiten over a float32 recording read and written through `io`, with
+ * the reference's two passes over the input (p_whiten.cpp:64-118 reads every
+ * chunk for XXt, :153-206 reads them again for the apply): the input is read
+ * twice, in increasing t0 each time.  Output as ms3gpu_whiten; every value
+ * equals the in-memory call's when a slab holds one slice of the covariance
+ * sum (about N / 56 timepoints at M = 384; N / 1184 at M <= 64), and differs
+ * otherwise only by the order of the FP64 covariance additions. */
+MS3GPU_API int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io,
+                                    const ms3gpu_whiten_opts* opts, void* stream);
 
 #ifdef __cplusplus
 }

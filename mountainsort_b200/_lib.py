@@ -17,6 +17,7 @@ ERR_INVALID = -1
 ERR_CUDA = -2
 ERR_UNSUPPORTED = -3
 ERR_NOMEM = -4
+ERR_IO = -5
 DTYPE_FLOAT32 = -3
 DTYPE_INT16 = -4
 
@@ -54,6 +55,21 @@ class Job(ctypes.Structure):
         ("bp", BandpassOpts),
         ("wh", WhitenOpts),
         ("status", ctypes.c_int32),
+    ]
+
+
+READ_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p)
+WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p)
+
+
+class StreamIO(ctypes.Structure):
+    """ms3gpu_stream_io: read / write callbacks of the streaming entry points."""
+    _fields_ = [
+        ("read", READ_FN),
+        ("read_ctx", ctypes.c_void_p),
+        ("write", WRITE_FN),
+        ("write_ctx", ctypes.c_void_p),
+        ("slab_bytes", ctypes.c_int64),
     ]
 
 
@@ -96,6 +112,10 @@ SIGNATURES = {
     "ms3gpu_mask_out_artifacts": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _i64, _vp, _vp, _vp]),
     "ms3gpu_detect_events": (ctypes.c_int, [_vp, _i64, _i64, _dbl, _dbl, ctypes.c_int32, _i64, _vp, _vp, _i64, _vp]),
     "ms3gpu_whiten_clips": (ctypes.c_int, [_vp, _i64, _i64, _i64, _vp, _dbl, ctypes.c_int32, _vp, _vp]),
+    "ms3gpu_bandpass_filter_stream": (ctypes.c_int, [_i64, _i64, ctypes.c_int32, ctypes.POINTER(StreamIO),
+                                                     ctypes.POINTER(BandpassOpts), _vp]),
+    "ms3gpu_whiten_stream": (ctypes.c_int, [_i64, _i64, ctypes.POINTER(StreamIO), ctypes.POINTER(WhitenOpts),
+                                            _vp]),
 }
 
 _lib = None

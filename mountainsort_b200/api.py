@@ -136,6 +136,81 @@ def whiten(X, quantization_unit=0.0, out=None, stream=None, precision="plain"):
     return out
 
 
+def _stream_io(M, source, sink, in_dtype, out_dtype, slab_bytes, errors):
+    """An ms3gpu_stream_io over Python callables: source(t0, nt) returns the
+    input timepoints [t0, t0 + nt) as an (nt, M) array; sink(t0, rows)
+    receives output timepoints as an (nt, M) array valid only during the
+    call.  An exception in either stops the call; it is kept in `errors`."""
+    in_ct = ctypes.c_int16 if np.dtype(in_dtype) == np.int16 else ctypes.c_float
+    out_ct = ctypes.c_int16 if np.dtype(out_dtype) == np.int16 else ctypes.c_float
+
+    def rd(_ctx, t0, nt, dst):
+        try:
+            block = np.ctypeslib.as_array(ctypes.cast(dst, ctypes.POINTER(in_ct)), shape=(nt, M))
+            block[...] = source(t0, nt)
+            return 0
+        except BaseException as e:  # noqa: BLE001 -- raised again after the call
+            errors.append(e)
+            return 1
+
+    def wr(_ctx, t0, nt, src):
+        try:
+            sink(t0, np.ctypeslib.as_array(ctypes.cast(src, ctypes.POINTER(out_ct)), shape=(nt, M)))
+            return 0
+        except BaseException as e:  # noqa: BLE001
+            errors.append(e)
+            return 1
+
+    return _lib.StreamIO(_lib.READ_FN(rd), None, _lib.WRITE_FN(wr), None, int(slab_bytes))
+
+
+def _run_stream(call, errors):
+    rc = call()
+    if errors:
+        raise errors[0]
+    check(rc)
+
+
+def bandpass_filter_stream(source, sink, M, N, samplerate, freq_min, freq_max, freq_wid=1000.0,
+                           quantization_unit=0.0, subsample_factor=1, num_threads=None, in_dtype=np.float32,
+                           slab_bytes=0, stream=None):
+    """ms3.bandpass_filter over a recording read and written block by block,
+    as the processor's chunk loop does (p_bandpass_filter.cpp:160-220).
+    source(t0, nt) returns input timepoints [t0, t0 + nt) as an (nt, M)
+    array (converted to in_dtype: float32, or int16 for an int16
+    recording); sink(t0, rows) receives output timepoints [t0, t0 + len(rows))
+    (float32, or int16 when quantization_unit != 0; the input's dtype when
+    freq_max == 0), in increasing t0.  The values equal bandpass_filter's.
+    slab_bytes: about how many input bytes one block holds (0 = 1 GiB)."""
+    L = _lib.load()
+    o = bandpass_opts(samplerate, freq_min, freq_max, freq_wid, quantization_unit, subsample_factor,
+                      num_threads)
+    i16 = np.dtype(in_dtype) == np.int16
+    if float(freq_max) == 0:
+        out_dt = np.int16 if i16 else np.float32
+    else:
+        out_dt = np.int16 if float(quantization_unit) != 0 else np.float32
+    errors = []
+    io = _stream_io(int(M), source, sink, np.int16 if i16 else np.float32, out_dt, slab_bytes, errors)
+    dt = _lib.DTYPE_INT16 if i16 else _lib.DTYPE_FLOAT32
+    _run_stream(lambda: L.ms3gpu_bandpass_filter_stream(int(M), int(N), dt, ctypes.byref(io), ctypes.byref(o),
+                                                        _stream_ptr(None, stream)), errors)
+
+
+def whiten_stream(source, sink, M, N, quantization_unit=0.0, slab_bytes=0, stream=None, precision="plain"):
+    """ms3.whiten over a float32 recording read block by block, twice (the
+    covariance pass, then the apply pass, p_whiten.cpp:64-206), written
+    block by block through sink (int16 when quantization_unit > 0).
+    Callbacks as in bandpass_filter_stream; the values equal whiten's."""
+    L = _lib.load()
+    o = WhitenOpts(float(quantization_unit), _PRECISION[precision])
+    errors = []
+    io = _stream_io(int(M), source, sink, np.float32, np.int16 if quantization_unit > 0 else np.float32,
+                    slab_bytes, errors)
+    _run_stream(lambda: L.ms3gpu_whiten_stream(int(M), int(N), ctypes.byref(io), ctypes.byref(o),
+                                               _stream_ptr(None, stream)), errors)
+
+
 def bandpass_whiten(X, samplerate, freq_min, freq_max, freq_wid=1000.0, num_threads=None,
                     quantization_unit=0.0, filt_out=None, out=None, want_filt=False, stream=None,
                     precision="plain"):

@@ -867,14 +867,23 @@ int64_t bandpass_chunk_size(int64_t M, int64_t num_threads) {
     return chunk_size;
 }
 
+void bandpass_output_rows(int64_t N, int64_t chunk, int sub, int64_t c_begin, int64_t c_end, int64_t& o0,
+                          int64_t& o1) {
+    o0 = std::min(N / sub, (c_begin * chunk) / sub);
+    o1 = std::min(N / sub, (c_end * chunk) / sub);
+}
+
 void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const BandpassParams& bp,
-                     cudaStream_t stream, int64_t c_begin, int64_t c_end, bool in_i16) {
+                     cudaStream_t stream, int64_t c_begin, int64_t c_end, bool in_i16, int64_t raw_row0,
+                     int64_t out_row0) {
     const int sub = bp.subsample_factor ? bp.subsample_factor : 1;
     if (sub < 1) throw_invalid("subsample_factor must be >= 1");
     const int64_t N2 = N / sub;
     const bool out_i16 = bp.quantization_unit != 0;
+    if (raw_row0 < 0 || out_row0 < 0) throw_invalid("negative slab origin");
     if (bp.freq_max == 0) {
         // p_bandpass_filter.cpp:117-119: the input file is copied unchanged.
+        if (raw_row0 != 0 || out_row0 != 0) throw_invalid("the copy (freq_max 0) takes whole recordings");
         if (M * N > 0)
             MS3_CUDA(cudaMemcpyAsync(out, raw, (in_i16 ? 2 : 4) * (size_t)(M * N), cudaMemcpyDeviceToDevice,
                                      stream));
@@ -894,7 +903,8 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
     // pair loads (float2, or short2 for int16 input) and float2 stores need
     // even M and aligned caller buffers
     g.in_i16 = in_i16 ? 1 : 0;
-    g.m_even = (M % 2 == 0) && ((uintptr_t)raw % (in_i16 ? 4 : 8) == 0) && ((uintptr_t)out % 8 == 0);
+    g.m_even = (M % 2 == 0) && ((uintptr_t)raw % (in_i16 ? 4 : 8) == 0) &&
+               (out_i16 || ((uintptr_t)out % 8 == 0));
     g.L = L;
     g.L1 = plan->L1;
     g.L2 = plan->L2;
@@ -951,10 +961,20 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
         }
     }
     // Gaps between subsampled chunks stay zero, as in the preallocated file.
-    if (sub > 1 && chunk % sub != 0 && c_begin == 0) {
-        const size_t esz = out_i16 ? 2 : 4;
-        MS3_CUDA(cudaMemsetAsync(out, 0, esz * (size_t)(M * N2), stream));
+    const size_t in_esz = in_i16 ? 2 : 4, out_esz = out_i16 ? 2 : 4;
+    if (sub > 1 && chunk % sub != 0) {
+        int64_t o0 = 0, o1 = 0;
+        bandpass_output_rows(N, chunk, sub, c_begin, c_end, o0, o1);
+        if (o0 < out_row0) throw_invalid("output slab starts after the windows' first row");
+        if (o1 > o0)
+            MS3_CUDA(cudaMemsetAsync(static_cast<char*>(out) + (size_t)((o0 - out_row0) * M) * out_esz, 0,
+                                     out_esz * (size_t)((o1 - o0) * M), stream));
     }
+    // The kernels index rows of the whole recording: a slab's pointers are
+    // moved back to where row 0 would be (only rows inside the slab are read
+    // or written).  Shifts are whole rows, so alignment is unchanged.
+    raw = reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(raw) - (uintptr_t)(raw_row0 * M) * in_esz);
+    out = reinterpret_cast<void*>(reinterpret_cast<uintptr_t>(out) - (uintptr_t)(out_row0 * M) * out_esz);
     int nsm = 0;
     {
         int dev = 0;

@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "ms3gpu.h"
 #include "pipeline.h"
+#include "stream.h"
 #include "whiten.h"
 
 namespace ms3gpu {
@@ -762,6 +763,37 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         pre.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
         bandpass_check_timeout(s);
+    });
+}
+
+namespace {
+void check_stream_io(const ms3gpu_stream_io* io, bool needs_write) {
+    if (!io) throw_invalid("stream io is NULL");
+    if (!io->read) throw_invalid("stream io has no read callback");
+    if (needs_write && !io->write) throw_invalid("stream io has no write callback");
+    if (io->slab_bytes < 0) throw_invalid("slab_bytes must be >= 0");
+}
+}  // namespace
+
+int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dtype, const ms3gpu_stream_io* io,
+                                  const ms3gpu_bandpass_opts* opts, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        BandpassParams p = to_params(opts);
+        check_stream_io(io, true);
+        if (in_dtype != MS3GPU_DTYPE_FLOAT32 && in_dtype != MS3GPU_DTYPE_INT16)
+            throw_invalid("in_dtype must be MS3GPU_DTYPE_FLOAT32 or MS3GPU_DTYPE_INT16");
+        bandpass_stream(M, N, in_dtype == MS3GPU_DTYPE_INT16, *io, p, as_stream(stream));
+    });
+}
+
+int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io, const ms3gpu_whiten_opts* opts,
+                         void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (!opts) throw_invalid("whiten opts is NULL");
+        check_stream_io(io, true);
+        whiten_stream(M, N, *io, opts->quantization_unit, check_precision(opts->precision), as_stream(stream));
     });
 }
 

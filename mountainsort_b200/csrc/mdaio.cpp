@@ -2,9 +2,12 @@
 #include "mdaio.h"
 
 #include <dirent.h>
+#include <fcntl.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <cerrno>
 
 #include <cstdio>
 #include <cstring>
@@ -357,6 +360,190 @@ bool read_timeseries_i16(const std::string& path, int64_t& M, int64_t& N, std::v
     N = h.dims.size() > 1 ? h.dims[1] : 1;
     data.resize((size_t)(M * N));
     if ((int64_t)std::fread(data.data(), 2, (size_t)(M * N), f.get()) != M * N) { err = "short read from " + path; return false; }
+    return true;
+}
+
+}  // namespace ms3io
+
+namespace ms3io {
+
+namespace {
+// pread / pwrite of the whole range (they may move fewer bytes per call)
+bool pread_all(int fd, void* dst, size_t n, int64_t off) {
+    char* p = static_cast<char*>(dst);
+    while (n > 0) {
+        const ssize_t r = ::pread(fd, p, n, (off_t)off);
+        if (r < 0 && errno == EINTR) continue;
+        if (r <= 0) return false;
+        p += r;
+        n -= (size_t)r;
+        off += r;
+    }
+    return true;
+}
+
+bool pwrite_all(int fd, const void* src, size_t n, int64_t off) {
+    const char* p = static_cast<const char*>(src);
+    while (n > 0) {
+        const ssize_t r = ::pwrite(fd, p, n, (off_t)off);
+        if (r < 0 && errno == EINTR) continue;
+        if (r <= 0) return false;
+        p += r;
+        n -= (size_t)r;
+        off += r;
+    }
+    return true;
+}
+}  // namespace
+
+RowReader::~RowReader() {
+    for (Seg& g : segs_)
+        if (g.fd >= 0) ::close(g.fd);
+}
+
+bool RowReader::open(const std::string& path, std::string& err) {
+    std::vector<std::string> files;
+    if (!input_files(path, files, err)) return false;
+    M_ = -1;
+    N_ = 0;
+    for (const std::string& f : files) {
+        MdaHeader h;
+        if (!read_header(f, h, err)) return false;
+        const int64_t m = h.dims[0], n = h.dims.size() > 1 ? h.dims[1] : 1;
+        if (M_ >= 0 && m != M_) {
+            err = "the files of " + path + " differ in channel count";
+            return false;
+        }
+        Seg g;
+        g.path = f;
+        g.offset = h.header_size;
+        g.t0 = N_;
+        g.n = n;
+        g.type = h.data_type;
+        g.bpe = h.bytes_per_entry;
+        g.fd = ::open(f.c_str(), O_RDONLY);
+        if (g.fd < 0) {
+            err = "cannot open " + f;
+            return false;
+        }
+        type_ = (M_ < 0 || type_ == h.data_type) ? h.data_type : 0;
+        segs_.push_back(g);
+        M_ = m;
+        N_ += n;
+    }
+    return true;
+}
+
+bool RowReader::read(int64_t t0, int64_t nt, int32_t as_type, void* dst, std::string& err) {
+    if (t0 < 0 || nt < 0 || t0 + nt > N_) {
+        err = "read outside the recording";
+        return false;
+    }
+    if (as_type != kFloat32 && !(as_type == kInt16 && type_ == kInt16)) {
+        err = "unsupported conversion for " + std::to_string(as_type);
+        return false;
+    }
+    const size_t out_bpe = as_type == kFloat32 ? 4 : 2;
+    for (const Seg& g : segs_) {
+        const int64_t a = std::max(t0, g.t0), b = std::min(t0 + nt, g.t0 + g.n);
+        if (a >= b) continue;
+        const int64_t count = (b - a) * M_;
+        const int64_t off = g.offset + (a - g.t0) * M_ * g.bpe;
+        char* out = static_cast<char*>(dst) + (size_t)((a - t0) * M_) * out_bpe;
+        if (g.type == as_type) {
+            if (!pread_all(g.fd, out, (size_t)count * out_bpe, off)) {
+                err = "short read from " + g.path;
+                return false;
+            }
+            continue;
+        }
+        // other types go through a block buffer, converted as mdaReadData does
+        const int64_t block = 1 << 20;
+        tmp_.resize((size_t)(block * g.bpe));
+        float* of = reinterpret_cast<float*>(out);
+        for (int64_t i = 0; i < count; i += block) {
+            const int64_t m = std::min(block, count - i);
+            if (!pread_all(g.fd, tmp_.data(), (size_t)(m * g.bpe), off + i * g.bpe)) {
+                err = "short read from " + g.path;
+                return false;
+            }
+            switch (g.type) {
+                case kUint8: convert(reinterpret_cast<const uint8_t*>(tmp_.data()), of + i, m); break;
+                case kFloat32: convert(reinterpret_cast<const float*>(tmp_.data()), of + i, m); break;
+                case kInt16: convert(reinterpret_cast<const int16_t*>(tmp_.data()), of + i, m); break;
+                case kInt32: convert(reinterpret_cast<const int32_t*>(tmp_.data()), of + i, m); break;
+                case kUint16: convert(reinterpret_cast<const uint16_t*>(tmp_.data()), of + i, m); break;
+                case kFloat64: convert(reinterpret_cast<const double*>(tmp_.data()), of + i, m); break;
+                default: err = "unsupported data type"; return false;
+            }
+        }
+    }
+    return true;
+}
+
+RowWriter::~RowWriter() {
+    if (fd_ >= 0) {
+        ::close(fd_);
+        std::remove(tmp_.c_str());
+    }
+}
+
+bool RowWriter::open(const std::string& path, int32_t data_type, int64_t M, int64_t N, std::string& err) {
+    path_ = path;
+    tmp_ = path + ".tmp";
+    M_ = M;
+    N_ = N;
+    bpe_ = bytes_per_entry(data_type);
+    std::remove(path.c_str());
+    fd_ = ::open(tmp_.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
+    if (fd_ < 0) {
+        err = "cannot open " + tmp_ + " for writing";
+        return false;
+    }
+    const bool use64 = (M > 2e9) || (N > 2e9);
+    unsigned char hdr[28];
+    const int32_t h3[3] = {data_type, (int32_t)bpe_, use64 ? -2 : 2};
+    std::memcpy(hdr, h3, 12);
+    if (use64) {
+        const int64_t d[2] = {M, N};
+        std::memcpy(hdr + 12, d, 16);
+        header_ = 28;
+    } else {
+        const int32_t d[2] = {(int32_t)M, (int32_t)N};
+        std::memcpy(hdr + 12, d, 8);
+        header_ = 20;
+    }
+    if (!pwrite_all(fd_, hdr, (size_t)header_, 0) || ::ftruncate(fd_, (off_t)(header_ + M * N * bpe_)) != 0) {
+        err = "cannot size " + tmp_;
+        return false;
+    }
+    return true;
+}
+
+bool RowWriter::write(int64_t t0, int64_t nt, const void* src, std::string& err) {
+    if (fd_ < 0 || t0 < 0 || nt < 0 || t0 + nt > N_) {
+        err = "write outside the output";
+        return false;
+    }
+    if (!pwrite_all(fd_, src, (size_t)(nt * M_ * bpe_), header_ + t0 * M_ * bpe_)) {
+        err = "write failed for " + tmp_;
+        return false;
+    }
+    return true;
+}
+
+bool RowWriter::commit(std::string& err) {
+    const int fd = fd_;
+    fd_ = -1;
+    if (fd < 0 || ::close(fd) != 0) {
+        std::remove(tmp_.c_str());
+        err = "write failed for " + tmp_;
+        return false;
+    }
+    if (std::rename(tmp_.c_str(), path_.c_str()) != 0) {
+        err = "cannot rename " + tmp_ + " to " + path_;
+        return false;
+    }
     return true;
 }
 

@@ -216,6 +216,44 @@ int32_t precision_of(const CLParams& clp) {
     return clp.str("_precision") == "mixed" ? MS3GPU_PRECISION_MIXED : MS3GPU_PRECISION_PLAIN;
 }
 
+// The processors' files as the streaming entry points read and write them:
+// rows of the input (converted to float32 unless kept as int16) and rows of
+// the output's .tmp file.
+struct StreamFiles {
+    ms3io::RowReader in;
+    ms3io::RowWriter out;
+    int32_t in_type = ms3io::kFloat32;
+    std::string err;
+};
+
+int read_rows_cb(void* ctx, int64_t t0, int64_t nt, void* dst) {
+    auto* f = static_cast<StreamFiles*>(ctx);
+    return f->in.read(t0, nt, f->in_type, dst, f->err) ? 0 : 1;
+}
+
+int write_rows_cb(void* ctx, int64_t t0, int64_t nt, const void* src) {
+    auto* f = static_cast<StreamFiles*>(ctx);
+    return f->out.write(t0, nt, src, f->err) ? 0 : 1;
+}
+
+// --_slab_mb=<MB> sets the rows read per block (not a reference parameter;
+// default 1024)
+ms3gpu_stream_io stream_io(StreamFiles& f, const CLParams& clp) {
+    ms3gpu_stream_io io{};
+    io.read = read_rows_cb;
+    io.read_ctx = &f;
+    io.write = write_rows_cb;
+    io.write_ctx = &f;
+    io.slab_bytes = (int64_t)(clp.num("_slab_mb", 0) * 1048576.0);
+    return io;
+}
+
+int stream_fail(const StreamFiles& f) {
+    std::string msg = ms3gpu_last_error();
+    if (!f.err.empty()) msg += ": " + f.err;
+    return fail(msg);
+}
+
 int run_bandpass(const CLParams& clp, bool requirements_only) {
     const std::string in = clp.str("timeseries"), out = clp.str("timeseries_out");
     ms3gpu_bandpass_opts o = bandpass_opts(clp);
@@ -242,24 +280,18 @@ int run_bandpass(const CLParams& clp, bool requirements_only) {
     int64_t Mo = 0, No = 0;
     int32_t dt = 0;
     if (ms3gpu_bandpass_output_dims(M, N, &o, &Mo, &No, &dt) != MS3GPU_OK) return fail(ms3gpu_last_error());
-    std::vector<unsigned char> Y((size_t)(Mo * No) * (dt == MS3GPU_DTYPE_INT16 ? 2 : 4));
     std::fprintf(stderr, "ms3gpu: bandpass %lld x %lld, chunk %lld (T=%d)\n", (long long)M, (long long)N,
                  (long long)ms3gpu_bandpass_chunk_size(M, o.num_threads), o.num_threads);
-    int rc;
-    if (dtype == ms3io::kInt16 && !ms3io::is_directory(in)) {
-        // an int16 recording goes to the GPU as int16 and is converted in the filter's loads
-        std::vector<int16_t> X16;
-        int64_t M1 = 0, N1 = 0;
-        if (!ms3io::read_timeseries_i16(in, M1, N1, X16, err)) return fail(err);
-        rc = ms3gpu_bandpass_filter_i16(X16.data(), M, N, Y.data(), &o, nullptr);
-    } else {
-        std::vector<float> X;
-        int64_t M1 = 0, N1 = 0;
-        if (!ms3io::read_timeseries_any_f32(in, M1, N1, X, err)) return fail(err);
-        rc = ms3gpu_bandpass_filter(X.data(), M, N, Y.data(), &o, nullptr);
-    }
-    if (rc != MS3GPU_OK) return fail(ms3gpu_last_error());
-    if (!ms3io::write_timeseries(out, dt, Mo, No, Y.data(), err)) return fail(err);
+    // the recording streams through the GPU in slabs of whole chunks; int16
+    // recordings go to the GPU as int16 and are converted in the filter's loads
+    StreamFiles f;
+    if (!f.in.open(in, err)) return fail(err);
+    f.in_type = f.in.data_type() == ms3io::kInt16 ? ms3io::kInt16 : ms3io::kFloat32;
+    if (!f.out.open(out, dt, Mo, No, err)) return fail(err);
+    const ms3gpu_stream_io io = stream_io(f, clp);
+    const int32_t in_dtype = f.in_type == ms3io::kInt16 ? MS3GPU_DTYPE_INT16 : MS3GPU_DTYPE_FLOAT32;
+    if (ms3gpu_bandpass_filter_stream(M, N, in_dtype, &io, &o, nullptr) != MS3GPU_OK) return stream_fail(f);
+    if (!f.out.commit(err)) return fail(err);
     return 0;
 }
 
@@ -281,13 +313,14 @@ int run_whiten(const CLParams& clp, bool requirements_only) {
         print_requirements(mb);
         return 0;
     }
-    std::vector<float> X;
-    int64_t M1 = 0, N1 = 0;
-    if (!ms3io::read_timeseries_any_f32(in, M1, N1, X, err)) return fail(err);
+    // two passes over the input, as the reference reads it (p_whiten.cpp:64-206)
+    StreamFiles f;
+    if (!f.in.open(in, err)) return fail(err);
     const bool i16 = o.quantization_unit > 0;
-    std::vector<unsigned char> Y((size_t)(M * N) * (i16 ? 2 : 4));
-    if (ms3gpu_whiten(X.data(), M, N, Y.data(), &o, nullptr) != MS3GPU_OK) return fail(ms3gpu_last_error());
-    if (!ms3io::write_timeseries(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    if (!f.out.open(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, err)) return fail(err);
+    const ms3gpu_stream_io io = stream_io(f, clp);
+    if (ms3gpu_whiten_stream(M, N, &io, &o, nullptr) != MS3GPU_OK) return stream_fail(f);
+    if (!f.out.commit(err)) return fail(err);
     return 0;
 }
 

@@ -509,12 +509,16 @@ CovPlan cov_plan(const float* X, int64_t M) {
     return p;
 }
 
+int64_t cov_tslice(const CovPlan& p, int64_t rows) {
+    if (rows <= 0) return kTT;
+    const int64_t target = std::max<int64_t>(1, (int64_t)(p.vec ? 8 : 4) * num_sms() / p.npairs);
+    const int64_t S = std::min<int64_t>(target, ceil_div(rows, kTT));
+    return ceil_div(ceil_div(rows, S), kTT) * kTT;
+}
+
 int64_t cov_slices(const CovPlan& p, int64_t rows) {
     if (rows <= 0) return 0;
-    const int64_t target = std::max<int64_t>(1, (int64_t)(p.vec ? 8 : 4) * num_sms() / p.npairs);
-    int64_t S = std::min<int64_t>(target, ceil_div(rows, kTT));
-    const int64_t tslice = ceil_div(ceil_div(rows, S), kTT) * kTT;
-    return ceil_div(rows, tslice);
+    return ceil_div(rows, cov_tslice(p, rows));
 }
 
 size_t cov_partials_bytes(const CovPlan& p, int64_t slices) {
@@ -525,7 +529,15 @@ void cov_partials(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPl
                   int64_t S, cudaStream_t stream) {
     const int64_t rows = r1 - r0;
     if (rows <= 0 || S <= 0) return;
-    const int64_t tslice = ceil_div(ceil_div(rows, S), kTT) * kTT;
+    cov_partials_sliced(X, M, r0, r1, p, partials, ceil_div(ceil_div(rows, S), kTT) * kTT, stream);
+}
+
+void cov_partials_sliced(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPlan& p, double* partials,
+                         int64_t tslice, cudaStream_t stream) {
+    const int64_t rows = r1 - r0;
+    if (rows <= 0) return;
+    if (tslice <= 0 || tslice % kTT != 0) throw_invalid("covariance slice length must be a multiple of 32");
+    const int64_t S = ceil_div(rows, tslice);
     if (p.vec)
         cov_partial8<<<dim3(p.npairs, (unsigned)S), 64, 0, stream>>>(X, M, r0, r1, p.nb, tslice, partials);
     else

@@ -22,6 +22,13 @@ int64_t cov_slices(const CovPlan& p, int64_t rows);
 size_t cov_partials_bytes(const CovPlan& p, int64_t slices);
 void cov_partials(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPlan& p, double* partials,
                   int64_t S, cudaStream_t stream);
+// The slice length covariance_device uses for `rows` rows (a multiple of 32),
+// and cov_partials with that length given: ceil((r1 - r0) / tslice) slices.
+// A recording streamed in slabs of whole slices, each slab's slices written
+// after the previous slab's, sums to the same XXt bit for bit.
+int64_t cov_tslice(const CovPlan& p, int64_t rows);
+void cov_partials_sliced(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPlan& p, double* partials,
+                         int64_t tslice, cudaStream_t stream);
 void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, int64_t N, double* XXt,
                 cudaStream_t stream);
 

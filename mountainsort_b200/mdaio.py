@@ -140,3 +140,45 @@ def timeseries_as_rows(X: np.ndarray) -> np.ndarray:
     (one row of M channels per timepoint), which is the memory layout the
     GPU kernels and the C ABI use.  No copy when X is Fortran-contiguous."""
     return np.asarray(X).T
+
+
+def timeseries_rows_view(path: str):
+    """(M, N, rows) of an M x N .mda timeseries file without reading it:
+    rows is a read-only (N, M) memory map of the data in the file's dtype."""
+    hdr = read_header_path(path)
+    M = hdr.dims[0]
+    N = hdr.dims[1] if len(hdr.dims) > 1 else 1
+    if M * N == 0:
+        return M, N, np.zeros((N, M), dtype=hdr.dtype)
+    return M, N, np.memmap(path, dtype=hdr.dtype, mode="r", offset=hdr.header_size, shape=(N, M))
+
+
+class TimeseriesWriter:
+    """An M x N timeseries written block by block into ``path.tmp``, sized in
+    full when opened (timepoints never written stay zero, like the
+    reference's preallocated file), renamed to ``path`` by close()
+    (``mda/diskwritemda.cpp:57-149,255-265``); abort() removes it."""
+
+    def __init__(self, path: str, dtype, M: int, N: int):
+        self.path, self.tmp = path, path + ".tmp"
+        dt = np.dtype(dtype)
+        hdr = MdaHeader(CODE_OF[dt], (M, N))
+        with open(self.tmp, "wb") as f:
+            write_header(f, hdr)
+            f.truncate(hdr.header_size + M * N * dt.itemsize)
+        self._rows = (np.memmap(self.tmp, dtype=dt, mode="r+", offset=hdr.header_size, shape=(N, M))
+                      if M * N > 0 else None)
+
+    def write(self, t0: int, rows: np.ndarray) -> None:
+        self._rows[t0:t0 + len(rows)] = rows
+
+    def close(self) -> None:
+        if self._rows is not None:
+            self._rows.flush()
+            self._rows = None
+        os.replace(self.tmp, self.path)
+
+    def abort(self) -> None:
+        self._rows = None
+        if os.path.exists(self.tmp):
+            os.remove(self.tmp)

@@ -68,18 +68,36 @@ def bandpass_filter(timeseries, timeseries_out, samplerate, freq_min, freq_max, 
             return False
         shutil.copyfile(timeseries, timeseries_out)
         return True
-    X = _read_rows(timeseries)
-    Y = api.bandpass_filter(X, samplerate, freq_min, freq_max, freq_wid, quantization_unit,
-                            subsample_factor, num_threads=_request_num_threads)
-    mdaio.writemda(Y.T, timeseries_out)
+    # the recording streams through the GPU block by block, as the
+    # processor's chunk loop reads it (p_bandpass_filter.cpp:160-220)
+    M, N, rows = mdaio.timeseries_rows_view(timeseries)
+    in_dt = np.int16 if rows.dtype == np.int16 else np.float32
+    sub = int(subsample_factor or 1)
+    out_dt = np.int16 if float(quantization_unit) != 0 else np.float32
+    out = mdaio.TimeseriesWriter(timeseries_out, out_dt, M, N // sub)
+    try:
+        api.bandpass_filter_stream(lambda t0, nt: rows[t0:t0 + nt], out.write, M, N, samplerate, freq_min,
+                                   freq_max, freq_wid, quantization_unit, sub, num_threads=_request_num_threads,
+                                   in_dtype=in_dt)
+    except BaseException:
+        out.abort()
+        raise
+    out.close()
     return True
 
 
 def whiten(timeseries, timeseries_out, quantization_unit=0) -> bool:
-    """ms3.whiten (p_whiten.cpp:45-206)."""
-    X = _read_rows(timeseries)
-    Y = api.whiten(X, quantization_unit=float(quantization_unit))
-    mdaio.writemda(Y.T, timeseries_out)
+    """ms3.whiten (p_whiten.cpp:45-206), reading the input twice like the
+    reference (the covariance pass, then the apply pass)."""
+    M, N, rows = mdaio.timeseries_rows_view(timeseries)
+    q = float(quantization_unit)
+    out = mdaio.TimeseriesWriter(timeseries_out, np.int16 if q > 0 else np.float32, M, N)
+    try:
+        api.whiten_stream(lambda t0, nt: rows[t0:t0 + nt], out.write, M, N, quantization_unit=q)
+    except BaseException:
+        out.abort()
+        raise
+    out.close()
     return True
 
 

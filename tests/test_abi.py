@@ -78,6 +78,39 @@ def test_invalid_arguments_rejected_before_device_work(call):
     assert _lib.last_error()
 
 
+def _io(read=True, write=True, slab_bytes=0):
+    rd = _lib.READ_FN(lambda c, t0, nt, d: 0) if read else _lib.READ_FN()
+    wr = _lib.WRITE_FN(lambda c, t0, nt, s: 0) if write else _lib.WRITE_FN()
+    return _lib.StreamIO(rd, None, wr, None, slab_bytes)
+
+
+@pytest.mark.parametrize("make", [
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, _lib.DTYPE_FLOAT32, None, ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, _lib.DTYPE_FLOAT32, ctypes.byref(_io(read=False)),
+                                                    ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, _lib.DTYPE_FLOAT32, ctypes.byref(_io(write=False)),
+                                                    ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, -7, ctypes.byref(_io()), ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, _lib.DTYPE_FLOAT32, ctypes.byref(_io(slab_bytes=-1)),
+                                                    ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(-4, 10, _lib.DTYPE_FLOAT32, ctypes.byref(_io()),
+                                                    ctypes.byref(o), None),
+    lambda L, o, w: L.ms3gpu_bandpass_filter_stream(4, 10, _lib.DTYPE_FLOAT32, ctypes.byref(_io()), None, None),
+    lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, None, ctypes.byref(w), None),
+    lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io()), None, None),
+    lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io(write=False)), ctypes.byref(w), None),
+    lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io()), ctypes.byref(_lib.WhitenOpts(0, 7)), None),
+])
+def test_stream_arguments_rejected_before_device_work(make):
+    """The streaming entry points check their callbacks, dtype, slab size,
+    shape and options before any CUDA call or callback."""
+    L = _lib.load()
+    o = api.bandpass_opts(30000, 300, 6000, 1000, 0, 1, 16)
+    w = _lib.WhitenOpts(0, 0)
+    assert make(L, o, w) == _lib.ERR_INVALID
+    assert _lib.last_error()
+
+
 def test_bad_num_threads_rejected():
     L = _lib.load()
     o = api.bandpass_opts(30000, 300, 6000, 1000, 0, 1, 16)

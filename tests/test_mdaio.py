@@ -92,3 +92,36 @@ def test_atomic_write_leaves_no_tmp(tmp_path):
     p = str(tmp_path / "a.mda")
     mdaio.writemda(np.zeros((2, 3), np.float32), p)
     assert os.path.exists(p) and not os.path.exists(p + ".tmp")
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.int16])
+def test_rows_view_and_block_writer(tmp_path, dt):
+    """The streaming processors' file access: a memory map of an input's
+    rows, and an output written block by block into a preallocated .tmp file
+    (unwritten timepoints zero), renamed when closed or removed when aborted."""
+    M, N = 5, 1001
+    X = (np.arange(M * N).reshape(N, M) % 3000).astype(dt)
+    src = str(tmp_path / "in.mda")
+    mdaio.writemda(X.T, src)
+    m, n, rows = mdaio.timeseries_rows_view(src)
+    assert (m, n) == (M, N) and rows.dtype == dt
+    np.testing.assert_array_equal(rows[10:20], X[10:20])
+    out = str(tmp_path / "out.mda")
+    w = mdaio.TimeseriesWriter(out, dt, M, N)
+    assert os.path.exists(out + ".tmp") and not os.path.exists(out)
+    w.write(0, X[:400])
+    w.write(600, X[600:])
+    w.close()
+    assert not os.path.exists(out + ".tmp")
+    Y = mdaio.readmda(out).T
+    np.testing.assert_array_equal(Y[:400], X[:400])
+    np.testing.assert_array_equal(Y[600:], X[600:])
+    assert not Y[400:600].any()
+    w = mdaio.TimeseriesWriter(str(tmp_path / "gone.mda"), dt, M, N)
+    w.abort()
+    assert not os.path.exists(str(tmp_path / "gone.mda.tmp"))
+    # an empty timeseries is a header only
+    e = str(tmp_path / "empty.mda")
+    w = mdaio.TimeseriesWriter(e, dt, M, 0)
+    w.close()
+    assert mdaio.readmda(e).shape == (M, 0)
