@@ -66,7 +66,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             print(r.stdout + r.stderr)
         os.replace(LIB + ".tmp", LIB)
     if force or not _newer(EXE, deps + [LIB]):
-        cmd = [_cxx(), "-O2", "-std=c++17", "-I", INCLUDE, "-I", CSRC, "-o", EXE + ".tmp",
+        cmd = [_cxx(), "-O2", "-std=c++17", "-pthread", "-I", INCLUDE, "-I", CSRC, "-o", EXE + ".tmp",
                *[os.path.join(CSRC, s) for s in EXE_SOURCES], "-L", HERE, "-l:libms3gpu.so",
                "-Wl,-rpath,$ORIGIN"]
         if verbose:

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "whiten.h"
@@ -361,6 +362,136 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
     }
 }
 
+// The same power iteration with the working matrix in registers, for M up
+// to 128 * RPW (8 CTAs x 16 warps x RPW rows) and 32 * CPL columns: lane l
+// of a warp holds its RPW rows at columns l + 32 j.  Every sum is formed in
+// the order pca_cluster forms it (per-lane column sums then the XOR
+// shuffle tree for a matvec row; 32-element warp trees summed in warp order
+// for a norm or a dot product), so components, sigma and W are identical.
+// Each warp forms the norm itself from the broadcast vector, so one
+// iteration is one matvec, one cluster barrier, the division and one block
+// barrier.  Matvec results alternate between two receive buffers: a CTA
+// writes buffer b of its peers only after every CTA has passed the barrier
+// that ended their reads of b.
+constexpr int kPcaWarps = kPcaThreads / 32;
+
+// Sum over n < M of f(n) in the order block_sum forms it when thread n
+// holds f(n): a 32-lane XOR tree per warp, then the warp totals in order.
+template <class F>
+__device__ __forceinline__ double warp_ordered_sum(int M, F f) {
+    const int l = threadIdx.x & 31;
+    double t = 0.0;
+    for (int c = 0; c * 32 < M; c++) {
+        const int n = c * 32 + l;
+        double v = n < M ? f(n) : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        t += v;
+    }
+    return t;
+}
+
+template <int RPW, int CPL>
+__global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* __restrict__ XXt, int M,
+                                                                   int num_iter, double* __restrict__ comps,
+                                                                   double* __restrict__ sigma) {
+    constexpr int kMaxM = 32 * CPL;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int CS = (int)cluster.num_blocks();
+    __shared__ double ybuf[2][kMaxM];  // matvec results, written by every CTA
+    __shared__ double vs[kMaxM];       // the normalised vector
+    __shared__ double vinit[kMaxM];
+    __shared__ double red[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int row0 = (rank * kPcaWarps + w) * RPW;
+
+    double A[RPW][CPL];
+#pragma unroll
+    for (int r = 0; r < RPW; r++)
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            const int m = row0 + r, n = l + 32 * j;
+            A[r][j] = (m < M && n < M) ? XXt[(size_t)m + (size_t)M * n] : 0.0;
+        }
+    // start vector sin(i+1), normalised (pca.cpp:546-549, 457-466)
+    for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = sin((double)(n + 1));
+    __syncthreads();
+    {
+        double part = 0.0;
+        for (int n = threadIdx.x; n < M; n += blockDim.x) part += vinit[n] * vinit[n];
+        const double nrm = sqrt(block_sum(part, red));
+        __syncthreads();
+        if (nrm != 0.0)
+            for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = vinit[n] / nrm;
+    }
+    __syncthreads();
+
+    // y = A v for this warp's rows, sent to every CTA's ybuf[b], then the barrier
+    auto matvec = [&](const double* v, int b) {
+        double s[RPW];
+#pragma unroll
+        for (int r = 0; r < RPW; r++) s[r] = 0.0;
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            const int n = l + 32 * j;
+            if (n < M) {
+                const double vn = v[n];
+#pragma unroll
+                for (int r = 0; r < RPW; r++) s[r] += A[r][j] * vn;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RPW; r++) {
+            for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
+            const int m = row0 + r;
+            if (m < M)
+                for (int d = l; d < CS; d += 32) cluster.map_shared_rank(&ybuf[b][0], d)[m] = s[r];
+        }
+        cluster.sync();
+    };
+
+    int b = 0;  // receive buffer of the next matvec (same sequence in every CTA)
+    for (int k = 0; k < M; k++) {
+        const double* v = vinit;
+        double sig = 0.0;
+        for (int it = 0; it < num_iter; it++) {
+            matvec(v, b);
+            const double* y = ybuf[b];
+            sig = sqrt(warp_ordered_sum(M, [&](int n) { return y[n] * y[n]; }));
+            for (int n = threadIdx.x; n < M; n += blockDim.x) vs[n] = sig != 0.0 ? y[n] / sig : y[n];
+            __syncthreads();
+            v = vs;
+            b ^= 1;
+        }
+        if (rank == 0) {
+            for (int n = threadIdx.x; n < M; n += blockDim.x) comps[(size_t)n + (size_t)M * k] = v[n];
+            if (threadIdx.x == 0) sigma[k] = sig;
+        }
+        // deflation: X <- X - v u' - u v' + (v'u) v v',  u = X v
+        matvec(v, b);
+        const double* u = ybuf[b];
+        b ^= 1;
+        const double alpha = warp_ordered_sum(M, [&](int n) { return v[n] * u[n]; });
+#pragma unroll
+        for (int r = 0; r < RPW; r++) {
+            const int m = row0 + r;
+            if (m >= M) continue;
+            const double vm = v[m], um = u[m];
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                const int n = l + 32 * j;
+                if (n < M) {
+                    const double sdef = __dadd_rn(__dmul_rn(vm, u[n]), __dmul_rn(um, v[n]));
+                    const double x = __dsub_rn(A[r][j], sdef);
+                    A[r][j] = __dadd_rn(x, __dmul_rn(alpha, __dmul_rn(vm, v[n])));
+                }
+            }
+        }
+        // vs is rewritten by the next component's first division only after
+        // its matvec's cluster barrier, which every thread reaches after this update
+    }
+}
+
 // W = (C D) C^T, D = diag(1/sqrt(sigma)) (0 where sigma == 0), in the
 // reference's order: tmp(m,l) = C(m,l) d_l (mult_AB with a diagonal,
 // pca.cpp:220-243), W(m,n) = sum_l tmp(m,l) C(n,l) (mult_ABtrans, :319-342).
@@ -630,6 +761,9 @@ void covariance_device_noalloc(const float* X, int64_t M, int64_t N, double* XXt
     MS3_LAUNCH_CHECK();
 }
 
+// pca_cluster launch: rows in shared memory across 8 or 16 CTAs, else in global memory.
+void pca_launch_smem(const double* XXt, int64_t M, double* comps, double* sigma, cudaStream_t stream);
+
 void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* comps, double* sigma,
                              cudaStream_t stream) {
     if (M <= 0) return;
@@ -638,6 +772,38 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
     if (!comps) { cbuf.alloc(sizeof(double) * (size_t)(M * M), stream); comps = cbuf.as<double>(); }
     if (!sigma) { sbuf.alloc(sizeof(double) * (size_t)M, stream); sigma = sbuf.as<double>(); }
 
+    // registers hold the working matrix up to 384 channels (MS3GPU_PCA_KERNEL=smem
+    // selects the shared-memory kernel, which gives the same values)
+    const char* pk = std::getenv("MS3GPU_PCA_KERNEL");
+    const bool force_smem = pk && std::string(pk) == "smem";
+    const char* force_global0 = std::getenv("MS3GPU_PCA_ROWS_GLOBAL");
+    if (!force_smem && !(force_global0 && force_global0[0] == '1') && M <= 384) {
+        auto kern = M <= 128 ? pca_cluster_reg<1, 4> : (M <= 256 ? pca_cluster_reg<2, 8> : pca_cluster_reg<3, 12>);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(8, 1, 1);
+        cfg.blockDim = dim3(kPcaThreads, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 8;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MS3_CUDA(cudaLaunchKernelEx(&cfg, kern, XXt, (int)M, 10, comps, sigma));
+        MS3_LAUNCH_CHECK();
+    } else {
+        pca_launch_smem(XXt, M, comps, sigma, stream);
+    }
+    const size_t wsm = sizeof(double) * (size_t)M;
+    if (wsm > 48 * 1024)
+        MS3_CUDA(cudaFuncSetAttribute(w_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    w_assemble<<<dim3((unsigned)ceil_div(M, 128), (unsigned)M), 128, wsm, stream>>>(comps, sigma, (int)M, W);
+    MS3_LAUNCH_CHECK();
+}
+
+void pca_launch_smem(const double* XXt, int64_t M, double* comps, double* sigma, cudaStream_t stream) {
     int dev = 0, max_optin = 0;
     MS3_CUDA(cudaGetDevice(&dev));
     MS3_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -676,11 +842,6 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     MS3_CUDA(cudaLaunchKernelEx(&cfg, pca_cluster, XXt, (int)M, R, 10, in_smem, xg.as<double>(), comps, sigma));
-    MS3_LAUNCH_CHECK();
-    const size_t wsm = sizeof(double) * (size_t)M;
-    if (wsm > 48 * 1024)
-        MS3_CUDA(cudaFuncSetAttribute(w_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
-    w_assemble<<<dim3((unsigned)ceil_div(M, 128), (unsigned)M), 128, wsm, stream>>>(comps, sigma, (int)M, W);
     MS3_LAUNCH_CHECK();
 }
 

@@ -150,6 +150,23 @@ def test_whitening_matrix_m500_cluster16(gpu_lib):
     assert rel(sig, sig64) <= 1e-8
 
 
+@pytest.mark.parametrize("M", [1, 2, 31, 33, 100, 128, 129, 200, 256, 257, 300, 383, 384])
+def test_whitening_matrix_register_kernel_matches_shared(gpu_lib, M):
+    # Up to 384 channels the working matrix lives in registers and every
+    # norm is formed per warp; the sums keep the shared-memory kernel's order,
+    # so components, sigma and W are bit-identical to it.
+    C = _cov(M, M + 7)
+    W_r, comps_r, sig_r = api.whitening_matrix(C, return_components=True)
+    os.environ["MS3GPU_PCA_KERNEL"] = "smem"
+    try:
+        W_s, comps_s, sig_s = api.whitening_matrix(C, return_components=True)
+    finally:
+        del os.environ["MS3GPU_PCA_KERNEL"]
+    np.testing.assert_array_equal(sig_r, sig_s)
+    np.testing.assert_array_equal(comps_r, comps_s)
+    np.testing.assert_array_equal(W_r, W_s)
+
+
 @pytest.mark.parametrize("M", [384, 700])
 def test_whitening_matrix_global_rows_match_shared(gpu_lib, M):
     # The global-memory variant (rows that do not fit shared memory) runs the
