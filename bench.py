@@ -177,6 +177,27 @@ def run_reference_arm(args, size):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- replicas
+
+def max_over_ranks(dist, x, device):
+    """The slowest rank's figure: every timing of a multi-GPU run is the
+    maximum over the ranks (all ranks take part, rank order does not matter)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, M, N, steps, ms_total):
+    """Whole-job Gch-samples/s of `world` replicas, each filtering and
+    whitening its own M x N recording `steps` times in ms_total (the max over
+    ranks)."""
+    return world * M * N * steps / (ms_total / 1e3) / 1e9
+
+
 # ----------------------------------------------------------------- GPU arm
 
 def main():
@@ -248,13 +269,9 @@ def main():
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    ms_total = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(dist, ev0.elapsed_time(ev1), dev)
     ms_step = ms_total / args.steps
-    value = world * M * N * args.steps / (ms_total / 1e3) / 1e9
+    value = replica_throughput(world, M, N, args.steps, ms_total)
 
     # ---- stage breakdown (same data, device pointers, CUDA events on the launching stream)
     stages = {}
@@ -322,11 +339,7 @@ def main():
         t1 = time.perf_counter()
         for _ in range(args.e2e_steps):
             ms.bandpass_whiten(raw_np, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=pre_np)
-        el = time.perf_counter() - t1
-        if dist:
-            t = torch.tensor([el], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(dist, time.perf_counter() - t1, dev)
         e2e = {"value": world * M * N * args.e2e_steps / el / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * M * N, "d2h_bytes_per_step": 4 * M * N,
                "ms_per_step": el / args.e2e_steps * 1e3, "steps": args.e2e_steps,
