@@ -935,7 +935,7 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
     g.nwin = c_end - c_begin;
     const int64_t units = g.nwin * g.ngroups;
     const size_t unit_bytes = (size_t)L * G * sizeof(float2);
-    const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 512) << 20;
+    const size_t budget = env_size("MS3GPU_BP_SCRATCH_MB", 4096) << 20;
     int64_t per_batch = std::max<int64_t>(1, (int64_t)(budget / unit_bytes));
     per_batch = std::min<int64_t>(per_batch, std::min<int64_t>(units, 65535));
 

@@ -197,3 +197,32 @@ def test_executable_streams_in_blocks(gpu_lib, tmp_path):
     # 1 MB blocks hold whole covariance slices (768 timepoints): the same sums
     np.testing.assert_array_equal(mdaio.readmda(pre).T, api.whiten(F))
     assert not os.path.exists(pre + ".tmp")
+
+
+def test_executable_streams_directories_of_mixed_and_int16_files(gpu_lib, tmp_path):
+    # a directory's files are concatenated in time; float64 / float32 parts
+    # are read as float32, an all-int16 directory goes to the GPU as int16
+    M, N = 32, 500000
+    X = synth.generate_numpy(M, N, K=6, seed=8)
+    X16 = np.clip(np.round(X / 0.195), -32768, 32767).astype(np.int16)
+    cuts = [0, 130000, 131000, 500000]
+    mixed, ints = tmp_path / "mixed", tmp_path / "ints"
+    mixed.mkdir()
+    ints.mkdir()
+    for k, dt in enumerate([np.float64, np.float32, np.float64]):
+        part = X[cuts[k]:cuts[k + 1]]
+        mdaio.writemda(part.astype(dt).T, str(mixed / f"p{k}.mda"))
+        mdaio.writemda(X16[cuts[k]:cuts[k + 1]].T, str(ints / f"p{k}.mda"))
+    args = ["--samplerate=30000", "--freq_min=300", "--freq_max=6000", "--_request_num_threads=16", "--_slab_mb=8"]
+    for d, ref_in in [(mixed, X.astype(np.float64).astype(np.float32)), (ints, X16)]:
+        out = str(tmp_path / f"{d.name}_filt.mda")
+        r = _run("ms3.bandpass_filter", f"--timeseries={d}", f"--timeseries_out={out}", *args)
+        assert r.returncode == 0, r.stderr
+        ref = api.bandpass_filter(ref_in, FS, FMIN, FMAX, FWID, num_threads=16)
+        np.testing.assert_array_equal(mdaio.readmda(out).T, ref)
+    # whiten of a directory input streams it twice
+    pre = str(tmp_path / "pre.mda")
+    r = _run("ms3.whiten", f"--timeseries={mixed}", f"--timeseries_out={pre}", "--quantization_unit=0.1",
+             "--_slab_mb=8")
+    assert r.returncode == 0, r.stderr
+    np.testing.assert_array_equal(mdaio.readmda(pre).T, api.whiten(X.astype(np.float32), quantization_unit=0.1))
