@@ -318,6 +318,37 @@ MS3GPU_API int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dt
 MS3GPU_API int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io,
                                     const ms3gpu_whiten_opts* opts, void* stream);
 
+/* Time sharding.  The recording's windows (chunks of ms3gpu_bandpass_chunk_size
+ * timepoints) are independent, and the covariance is a sum over time, so the
+ * path splits along time across GPUs with one exchange: every GPU filters its
+ * own windows, sums x x^T over its own filtered timepoints, the M x M sums are
+ * added over the GPUs (a collective of the caller's choice), every GPU forms
+ * W from the total divided by N - 1 (ms3gpu_whitening_matrix: deterministic,
+ * so identical everywhere) and applies it to its own timepoints
+ * (ms3gpu_apply_whitening_matrix).  Whitened values equal the one-GPU call's
+ * up to the grouping of the FP64 covariance additions.
+ *
+ * ms3gpu_bandpass_filter_windows: p_bandpass_filter's chunk loop
+ * (p_bandpass_filter.cpp:160-220) restricted to windows [c_begin, c_end) of
+ * an M x N recording, on a slab: `timeseries` holds `rows` timepoints starting
+ * at timepoint row0 (in_dtype MS3GPU_DTYPE_FLOAT32 or MS3GPU_DTYPE_INT16), and
+ * must cover the windows' reads [c_begin*chunk - 60000, c_end*chunk + 60000)
+ * clipped to [0, N); `timeseries_out` holds out_rows output timepoints from
+ * out_row0 and must cover [c_begin*chunk, c_end*chunk) / subsample_factor
+ * clipped to N / subsample_factor.  Output values equal the whole-recording
+ * call's; other rows of timeseries_out are left as they are.  freq_max == 0
+ * is MS3GPU_ERR_INVALID (the copy takes whole recordings). */
+MS3GPU_API int ms3gpu_bandpass_filter_windows(const void* timeseries, int32_t in_dtype, int64_t M, int64_t N,
+                                              int64_t row0, int64_t rows, int64_t c_begin, int64_t c_end,
+                                              void* timeseries_out, int64_t out_row0, int64_t out_rows,
+                                              const ms3gpu_bandpass_opts* opts, void* stream);
+
+/* Whiten pass 1 (p_whiten.cpp:64-118) over one shard of timepoints without
+ * the division: XXt_sum = sum over the N timepoints of x_t x_t^T, M x M
+ * doubles. */
+MS3GPU_API int ms3gpu_whiten_covariance_sum(const float* timeseries, int64_t M, int64_t N, double* XXt_sum,
+                                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -766,6 +766,75 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
     });
 }
 
+int ms3gpu_bandpass_filter_windows(const void* timeseries, int32_t in_dtype, int64_t M, int64_t N, int64_t row0,
+                                   int64_t rows, int64_t c_begin, int64_t c_end, void* timeseries_out,
+                                   int64_t out_row0, int64_t out_rows, const ms3gpu_bandpass_opts* opts,
+                                   void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        BandpassParams p = to_params(opts);
+        if (in_dtype != MS3GPU_DTYPE_FLOAT32 && in_dtype != MS3GPU_DTYPE_INT16)
+            throw_invalid("in_dtype must be MS3GPU_DTYPE_FLOAT32 or MS3GPU_DTYPE_INT16");
+        if (p.freq_max == 0) throw_invalid("freq_max 0 copies whole recordings: use ms3gpu_bandpass_filter");
+        const int64_t chunk = bandpass_chunk_size(M, p.num_threads);
+        const int64_t nchunks = N > 0 ? ceil_div(N, chunk) : 0;
+        if (c_begin < 0 || c_end > nchunks || c_begin > c_end)
+            throw_invalid("windows [" + std::to_string(c_begin) + ", " + std::to_string(c_end) + ") outside [0, " +
+                          std::to_string(nchunks) + ")");
+        if (c_begin == c_end || M == 0) return;
+        const int sub = p.subsample_factor;
+        const int64_t need0 = std::max<int64_t>(0, c_begin * chunk - 60000);
+        const int64_t need1 = std::min<int64_t>(N, c_end * chunk + 60000);
+        if (row0 < 0 || rows < 0 || row0 > need0 || row0 + rows < need1)
+            throw_invalid("input rows [" + std::to_string(row0) + ", " + std::to_string(row0 + rows) +
+                          ") do not hold the windows' rows [" + std::to_string(need0) + ", " +
+                          std::to_string(need1) + ")");
+        int64_t o0 = 0, o1 = 0;
+        bandpass_output_rows(N, chunk, sub, c_begin, c_end, o0, o1);
+        if (out_row0 < 0 || out_rows < 0 || out_row0 > o0 || out_row0 + out_rows < o1)
+            throw_invalid("output rows [" + std::to_string(out_row0) + ", " + std::to_string(out_row0 + out_rows) +
+                          ") do not hold the windows' output rows [" + std::to_string(o0) + ", " +
+                          std::to_string(o1) + ")");
+        const bool in_i16 = in_dtype == MS3GPU_DTYPE_INT16;
+        const size_t in_bytes = (in_i16 ? 2 : 4) * (size_t)(rows * M);
+        const size_t out_bytes = (p.quantization_unit != 0 ? 2 : 4) * (size_t)(out_rows * M);
+        require(timeseries, "timeseries", in_bytes > 0);
+        require(timeseries_out, "timeseries_out", out_bytes > 0);
+        cudaStream_t s = as_stream(stream);
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(timeseries_out, out_bytes, s);
+        // rows of the output buffer outside the windows' rows keep what the caller had there
+        if (out.host && out_bytes) MS3_CUDA(cudaMemcpyAsync(out.ptr, timeseries_out, out_bytes, cudaMemcpyHostToDevice, s));
+        bandpass_device(in.ptr, M, N, out.ptr, p, s, c_begin, c_end, in_i16, row0, out_row0);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+        bandpass_check_timeout(s);
+    });
+}
+
+int ms3gpu_whiten_covariance_sum(const float* timeseries, int64_t M, int64_t N, double* XXt_sum, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        require(XXt_sum, "XXt_sum", M > 0);
+        cudaStream_t s = as_stream(stream);
+        const size_t in_bytes = sizeof(float) * (size_t)(M * N);
+        require(timeseries, "timeseries", in_bytes > 0);
+        if (M == 0) return;
+        InView in;
+        stage_in(in, timeseries, in_bytes, s);
+        OutView out;
+        out.setup(XXt_sum, sizeof(double) * (size_t)(M * M), s);
+        if (N == 0)
+            MS3_CUDA(cudaMemsetAsync(out.ptr, 0, sizeof(double) * (size_t)(M * M), s));
+        else
+            covariance_sum_device(static_cast<const float*>(in.ptr), M, N, static_cast<double*>(out.ptr), s);
+        out.finish(s);
+        MS3_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 namespace {
 void check_stream_io(const ms3gpu_stream_io* io, bool needs_write) {
     if (!io) throw_invalid("stream io is NULL");

@@ -687,6 +687,15 @@ void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, 
     MS3_LAUNCH_CHECK();
 }
 
+void covariance_sum_device(const float* X, int64_t M, int64_t N, double* XXt_sum, cudaStream_t stream) {
+    if (M <= 0) return;
+    const CovPlan p = cov_plan(X, M);
+    const int64_t S = cov_slices(p, N);
+    DevBuf partials(cov_partials_bytes(p, S), stream);
+    cov_partials(X, M, 0, N, p, partials.as<double>(), S, stream);
+    cov_finish(partials.as<double>(), S, p, M, /*N=*/1, XXt_sum, stream);  // N <= 1: no division
+}
+
 void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream) {
     if (M <= 0) return;
     const CovPlan p = cov_plan(X, M);

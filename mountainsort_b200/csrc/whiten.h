@@ -9,6 +9,9 @@ namespace ms3gpu {
 
 // XXt (M x M doubles, column-major) = sum_t x_t x_t^T / (N-1 if N > 1).
 void covariance_device(const float* X, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
+// The same sum over the N rows of X without the division (one shard's part
+// of a recording whose rows are spread over several GPUs).
+void covariance_sum_device(const float* X, int64_t M, int64_t N, double* XXt_sum, cudaStream_t stream);
 
 // The covariance in pieces, for callers that stream the rows in: partial
 // tiles of rows [r0, r1) go to `S` slices of a partials buffer; cov_finish

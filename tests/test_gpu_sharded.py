@@ -1,0 +1,119 @@
+"""The time-sharded filter + whiten on the GPU.  With one GPU the ranks are
+emulated one after another (each rank's kernels run alone; the exchange is
+the rank-order sum done here), and two gloo ranks share the GPU for the
+process-group form (their only wait on each other is the host-side
+all-gather).
+
+Gates: every rank's filtered timepoints equal the one-GPU call's bit for
+bit; one rank gives the one-GPU whitened output bit for bit; 2 and 3 ranks
+agree with it to relative L2 <= 1e-6 (the FP64 covariance grouping) and with
+ref32 to <= 1e-5."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from mountainsort_b200 import api, sharded, synth
+from oracle import oracle64 as o64
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FS, FMIN, FMAX, FWID = 30000.0, 300.0, 6000.0, 1000.0
+
+
+def _emulate(X, world, T=16, q=0.0, precision="plain"):
+    N, M = X.shape
+    shards = [sharded.shard_of(M, N, T, world, r) for r in range(world)]
+    filts = [sharded.filter_windows(X[s.in_row0:s.in_row1], s, M, N, FS, FMIN, FMAX, FWID, T) for s in shards]
+    total = None
+    for f in filts:  # the exchange: sums added in rank order
+        part = sharded.covariance_sum(f)
+        total = part.copy() if total is None else total + part
+    W = sharded.whitening_from_sum(total, N)
+    pres = [api.apply_whitening_matrix(f, W, q, precision=precision) for f in filts]
+    return shards, np.concatenate(filts), np.concatenate(pres)
+
+
+@pytest.mark.parametrize("M,N", [(32, 1_000_000), (384, 700_000)])
+def test_emulated_ranks_match_one_gpu(gpu_lib, ref32, M, N):
+    X = synth.generate_numpy(M, N, K=max(2, M // 8), seed=M + 3)
+    filt1 = api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre1 = api.whiten(filt1)
+    for world in [1, 2, 3]:
+        shards, filt, pre = _emulate(X, world)
+        np.testing.assert_array_equal(filt, filt1)
+        if world == 1:
+            np.testing.assert_array_equal(pre, pre1)
+        else:
+            assert o64.rel_l2(pre, pre1) <= 1e-6
+    if M == 32:
+        pre_ref, _, _ = ref32.whiten(ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16))
+        assert o64.rel_l2(pre, pre_ref) <= 1e-5
+
+
+def test_sharded_int16_slabs_and_covariance_sum(gpu_lib):
+    M, N = 64, 500_000
+    X = synth.generate_numpy(M, N, K=6, seed=12)
+    X16 = np.clip(np.round(X / 0.195), -32768, 32767).astype(np.int16)
+    filt1 = api.bandpass_filter(X16, FS, FMIN, FMAX, FWID, num_threads=16)
+    for world in [2, 4]:
+        for r in range(world):
+            s = sharded.shard_of(M, N, 16, world, r)
+            f = sharded.filter_windows(X16[s.in_row0:s.in_row1], s, M, N, FS, FMIN, FMAX, FWID, 16)
+            np.testing.assert_array_equal(f, filt1[s.out_row0:s.out_row1])
+    # the undivided sum over all timepoints, divided, is the covariance of one call
+    S = sharded.covariance_sum(filt1)
+    C = api.whiten_covariance(filt1)
+    np.testing.assert_array_equal(S / (N - 1), C)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q, M, N):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    sys.path.insert(0, ROOT)
+    from mountainsort_b200 import sharded as sh
+    from mountainsort_b200 import synth as sy
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        X = sy.generate_numpy(M, N, K=4, seed=21)
+        s = sh.shard_of(M, N, 16, world, rank)
+        shard, filt, pre = sh.bandpass_whiten_shard(X[s.in_row0:s.in_row1], M, N, FS, FMIN, FMAX, FWID, 16)
+        assert shard == s
+        q.put((rank, s.out_row0, s.out_row1, pre))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_process_group_ranks_on_one_gpu(gpu_lib):
+    # two processes, one GPU, gloo for the covariance exchange
+    M, N, world = 32, 600_000, 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q, M, N)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs)
+    pre = np.concatenate([r[3] for r in res])
+    X = synth.generate_numpy(M, N, K=4, seed=21)
+    _, _, pre_emul = _emulate(X, world)
+    np.testing.assert_array_equal(pre, pre_emul)
