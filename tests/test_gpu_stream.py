@@ -226,3 +226,23 @@ def test_executable_streams_directories_of_mixed_and_int16_files(gpu_lib, tmp_pa
              "--_slab_mb=8")
     assert r.returncode == 0, r.stderr
     np.testing.assert_array_equal(mdaio.readmda(pre).T, api.whiten(X.astype(np.float32), quantization_unit=0.1))
+
+
+@pytest.mark.parametrize("M,N", [(1, 50000), (3, 7), (16, 1), (8, 0), (0, 100)])
+def test_stream_edge_shapes(gpu_lib, M, N):
+    # one channel, recordings shorter than a window's halo, a single
+    # timepoint, empty recordings: the same values as the in-memory calls
+    X = (np.random.default_rng(M * 1000 + N).standard_normal((N, M)) * 20).astype(np.float32)
+    T = max(16, 187 // max(M, 1) + 1)
+    rec = Recorder(X, N, M, np.float32)
+    api.bandpass_filter_stream(rec.source, rec.sink, M, N, FS, FMIN, FMAX, FWID, num_threads=T, slab_bytes=1)
+    if M * N:
+        np.testing.assert_array_equal(rec.Y, api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=T))
+    else:
+        assert rec.reads == [] and not rec.written.any()
+    # one slab: the in-memory covariance slices (blocks smaller than a slice
+    # change only the FP64 summation order, tested above)
+    rec = Recorder(X, N, M, np.float32)
+    api.whiten_stream(rec.source, rec.sink, M, N)
+    if M * N:
+        np.testing.assert_array_equal(rec.Y, api.whiten(X))
