@@ -238,6 +238,11 @@ int write_rows_cb(void* ctx, int64_t t0, int64_t nt, const void* src) {
 
 // --_slab_mb=<MB> sets the rows read per block (not a reference parameter;
 // default 1024)
+int64_t slab_bytes(const CLParams& clp) {
+    const double mb = clp.num("_slab_mb", 0);
+    return mb > 0 ? (int64_t)(mb * 1048576.0) : (int64_t(1) << 30);
+}
+
 ms3gpu_stream_io stream_io(StreamFiles& f, const CLParams& clp) {
     ms3gpu_stream_io io{};
     io.read = read_rows_cb;
@@ -354,24 +359,49 @@ int run_compute_whitening_matrix(const CLParams& clp) {
             a = b + 1;
         }
     }
-    std::vector<std::vector<float>> data(it->second.size());
-    std::vector<const float*> ptrs;
-    std::vector<int64_t> Ns;
-    int64_t M = -1;
+    // The recordings are read block by block: each block's x x^T sum over the
+    // selected channels (ms3gpu_whiten_covariance_sum) is added into an FP64
+    // total, divided by (total timepoints - 1) as the reference divides
+    // (p_whiten.cpp:270-280), then the whitening matrix of that XXt.
     std::string err;
+    int64_t M = -1;
+    std::vector<ms3io::RowReader> readers(it->second.size());
     for (size_t i = 0; i < it->second.size(); i++) {
-        int64_t Mi = 0, Ni = 0;
-        if (!ms3io::read_timeseries_any_f32(it->second[i], Mi, Ni, data[i], err)) return fail(err);
-        if (M >= 0 && Mi != M) return fail("the recordings of timeseries_list differ in channel count");
-        M = Mi;
-        ptrs.push_back(data[i].data());
-        Ns.push_back(Ni);
+        if (!readers[i].open(it->second[i], err)) return fail(err);
+        if (M >= 0 && readers[i].M() != M) return fail("the recordings of timeseries_list differ in channel count");
+        M = readers[i].M();
     }
+    for (int32_t c : channels)
+        if (c < 1 || c > M)
+            return fail("channel " + std::to_string(c) + " outside 1.." + std::to_string(M) + " in channels");
     const int64_t M2 = channels.empty() ? M : (int64_t)channels.size();
+    std::vector<double> total((size_t)(M2 * M2), 0.0), part((size_t)(M2 * M2));
+    int64_t Ntot = 0;
+    const int64_t rows = std::max<int64_t>(1, slab_bytes(clp) / std::max<int64_t>(1, 4 * M));
+    std::vector<float> xb, sb;
+    for (ms3io::RowReader& r : readers) {
+        const int64_t Ni = r.N();
+        for (int64_t t = 0; t < Ni && M2 > 0; t += rows) {
+            const int64_t nt = std::min(rows, Ni - t);
+            xb.resize((size_t)(nt * M));
+            if (!r.read(t, nt, ms3io::kFloat32, xb.data(), err)) return fail(err);
+            const float* blk = xb.data();
+            if (!channels.empty()) {
+                sb.resize((size_t)(nt * M2));
+                for (int64_t k = 0; k < nt; k++)
+                    for (int64_t j = 0; j < M2; j++) sb[(size_t)(k * M2 + j)] = xb[(size_t)(k * M + channels[(size_t)j] - 1)];
+                blk = sb.data();
+            }
+            if (ms3gpu_whiten_covariance_sum(blk, M2, nt, part.data(), nullptr) != MS3GPU_OK)
+                return fail(ms3gpu_last_error());
+            for (size_t e = 0; e < total.size(); e++) total[e] += part[e];
+        }
+        Ntot += Ni;
+    }
+    if (Ntot > 1)
+        for (double& v : total) v /= (double)(Ntot - 1);
     std::vector<double> W((size_t)(M2 * M2));
-    if (ms3gpu_compute_whitening_matrix(ptrs.data(), Ns.data(), (int32_t)ptrs.size(), M,
-                                        channels.empty() ? nullptr : channels.data(), (int32_t)channels.size(),
-                                        W.data(), nullptr) != MS3GPU_OK)
+    if (M2 > 0 && ms3gpu_whitening_matrix(total.data(), M2, W.data(), nullptr, nullptr, nullptr) != MS3GPU_OK)
         return fail(ms3gpu_last_error());
     // Mda::write64 (float64)
     if (!ms3io::write_array(out, ms3io::kFloat64, {M2, M2}, W.data(), err)) return fail(err);
@@ -383,16 +413,29 @@ int run_apply_whitening_matrix(const CLParams& clp) {
     const std::string in = clp.str("timeseries"), wpath = clp.str("whitening_matrix"), out = clp.str("timeseries_out");
     const double q = clp.num("quantization_unit", 0);
     std::string err;
-    std::vector<float> X;
-    int64_t M = 0, N = 0;
-    if (!ms3io::read_timeseries_any_f32(in, M, N, X, err)) return fail(err);
+    ms3io::RowReader rd;
+    if (!rd.open(in, err)) return fail(err);
+    const int64_t M = rd.M(), N = rd.N();
     std::vector<double> W;
     if (!read_whitening_matrix(wpath, M, W, err)) return fail(err);
     const bool i16 = q > 0;
-    std::vector<unsigned char> Y((size_t)(M * N) * (i16 ? 2 : 4));
-    if (ms3gpu_apply_whitening_matrix(X.data(), M, N, W.data(), q, precision_of(clp), Y.data(), nullptr) != MS3GPU_OK)
-        return fail(ms3gpu_last_error());
-    if (!ms3io::write_timeseries(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    ms3io::RowWriter wr;
+    if (!wr.open(out, i16 ? ms3io::kInt16 : ms3io::kFloat32, M, N, err)) return fail(err);
+    // block by block: the apply is per timepoint, so the values are those of one call
+    const int64_t rows = std::max<int64_t>(1, slab_bytes(clp) / std::max<int64_t>(1, 4 * M));
+    std::vector<float> xb;
+    std::vector<unsigned char> yb;
+    for (int64_t t = 0; t < N && M > 0; t += rows) {
+        const int64_t nt = std::min(rows, N - t);
+        xb.resize((size_t)(nt * M));
+        yb.resize((size_t)(nt * M) * (i16 ? 2 : 4));
+        if (!rd.read(t, nt, ms3io::kFloat32, xb.data(), err)) return fail(err);
+        if (ms3gpu_apply_whitening_matrix(xb.data(), M, nt, W.data(), q, precision_of(clp), yb.data(), nullptr) !=
+            MS3GPU_OK)
+            return fail(ms3gpu_last_error());
+        if (!wr.write(t, nt, yb.data(), err)) return fail(err);
+    }
+    if (!wr.commit(err)) return fail(err);
     return 0;
 }
 

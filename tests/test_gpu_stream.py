@@ -246,3 +246,35 @@ def test_stream_edge_shapes(gpu_lib, M, N):
     api.whiten_stream(rec.source, rec.sink, M, N)
     if M * N:
         np.testing.assert_array_equal(rec.Y, api.whiten(X))
+
+
+def test_executable_whitening_matrix_processors_in_blocks(gpu_lib, ref32, tmp_path):
+    # ms3.compute_whitening_matrix sums x x^T block by block over the list;
+    # ms3.apply_whitening_matrix whitens block by block (values of one call)
+    M = 16
+    A = api.bandpass_filter(synth.generate_numpy(M, 300000, K=4, seed=31), FS, FMIN, FMAX, FWID, num_threads=16)
+    B = api.bandpass_filter(synth.generate_numpy(M, 170001, K=4, seed=32), FS, FMIN, FMAX, FWID, num_threads=16)
+    pa, pb, pw, po = (str(tmp_path / n) for n in ("a.mda", "b.mda", "W.mda", "o.mda"))
+    mdaio.writemda(A.T, pa)
+    mdaio.writemda(B.T, pb)
+    for chans, sel in [("", list(range(M))), ("--channels=3,1,16,8", [2, 0, 15, 7])]:
+        args = ["ms3.compute_whitening_matrix", f"--timeseries_list={pa}", "--timeseries_list", pb,
+                f"--whitening_matrix_out={pw}", "--_slab_mb=1"] + ([chans] if chans else [])
+        r = _run(*args)
+        assert r.returncode == 0, r.stderr
+        W = mdaio.readmda(pw)
+        W_mem = api.compute_whitening_matrix([A, B], channels=[c + 1 for c in sel] if chans else None)
+        assert o64.rel_l2(W, W_mem) <= 1e-9
+        W_ref, _ = ref32.compute_whitening_matrix([A, B], channels=[c + 1 for c in sel] if chans else None)
+        assert o64.rel_l2(W, W_ref) <= 1e-6
+    r = _run("ms3.compute_whitening_matrix", f"--timeseries_list={pa}", f"--whitening_matrix_out={pw}",
+             "--channels=0,2")
+    assert r.returncode != 0
+    # the apply with the all-channel W, in 1 MB blocks, int16 output
+    r = _run("ms3.compute_whitening_matrix", f"--timeseries_list={pa}", f"--whitening_matrix_out={pw}")
+    assert r.returncode == 0, r.stderr
+    W = mdaio.readmda(pw)
+    r = _run("ms3.apply_whitening_matrix", f"--timeseries={pa}", f"--whitening_matrix={pw}",
+             f"--timeseries_out={po}", "--quantization_unit=0.05", "--_slab_mb=1")
+    assert r.returncode == 0, r.stderr
+    np.testing.assert_array_equal(mdaio.readmda(po).T, api.apply_whitening_matrix(A, W, quantization_unit=0.05))
