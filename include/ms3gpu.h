@@ -318,6 +318,14 @@ MS3GPU_API int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dt
 MS3GPU_API int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io,
                                     const ms3gpu_whiten_opts* opts, void* stream);
 
+/* ms3.mask_out_artifacts over a float32 recording read and written through
+ * `io`: the input is read twice (the interval norms, then the masked copy),
+ * in blocks of whole intervals.  Output and *timepoints_kept equal
+ * ms3gpu_mask_out_artifacts'. */
+MS3GPU_API int ms3gpu_mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int64_t interval_size,
+                                                const ms3gpu_stream_io* io, int64_t* timepoints_kept,
+                                                void* stream);
+
 /* Time sharding.  The recording's windows (chunks of ms3gpu_bandpass_chunk_size
  * timepoints) are independent, and the covariance is a sum over time, so the
  * path splits along time across GPUs with one exchange: every GPU filters its

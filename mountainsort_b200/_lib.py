@@ -119,6 +119,8 @@ SIGNATURES = {
     "ms3gpu_bandpass_filter_windows": (ctypes.c_int, [_vp, ctypes.c_int32, _i64, _i64, _i64, _i64, _i64, _i64,
                                                       _vp, _i64, _i64, ctypes.POINTER(BandpassOpts), _vp]),
     "ms3gpu_whiten_covariance_sum": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp]),
+    "ms3gpu_mask_out_artifacts_stream": (ctypes.c_int, [_i64, _i64, _dbl, _i64, ctypes.POINTER(StreamIO), _vp,
+                                                        _vp]),
 }
 
 _lib = None

@@ -211,6 +211,21 @@ def whiten_stream(source, sink, M, N, quantization_unit=0.0, slab_bytes=0, strea
                                                _stream_ptr(None, stream)), errors)
 
 
+def mask_out_artifacts_stream(source, sink, M, N, threshold=6.0, interval_size=2000, slab_bytes=0, stream=None):
+    """ms3.mask_out_artifacts over a float32 recording read block by block,
+    twice (the interval norms, then the masked copy), written through sink.
+    Callbacks as in bandpass_filter_stream.  Returns the timepoints kept; the
+    values equal mask_out_artifacts'."""
+    L = _lib.load()
+    errors = []
+    io = _stream_io(int(M), source, sink, np.float32, np.float32, slab_bytes, errors)
+    kept = ctypes.c_int64()
+    _run_stream(lambda: L.ms3gpu_mask_out_artifacts_stream(int(M), int(N), float(threshold), int(interval_size),
+                                                           ctypes.byref(io), ctypes.byref(kept),
+                                                           _stream_ptr(None, stream)), errors)
+    return kept.value
+
+
 def bandpass_whiten(X, samplerate, freq_min, freq_max, freq_wid=1000.0, num_threads=None,
                     quantization_unit=0.0, filt_out=None, out=None, want_filt=False, stream=None,
                     precision="plain"):

@@ -65,12 +65,13 @@ __global__ void artifact_flags(const double* __restrict__ norms, int64_t M, int6
         if (norms[i * M + m] > limit) exceed[i] = 1;
 }
 
-// out(m, t) = x(m, t) where interval t / I is kept, else 0
+// out(m, t) = x(m, t) where interval t / I is kept, else 0; X and out hold
+// the N timepoints from t0
 __global__ void artifact_write(const float* __restrict__ X, int64_t M, int64_t N, int64_t I, int64_t nint,
-                               const int* __restrict__ exceed, float* __restrict__ out) {
+                               const int* __restrict__ exceed, float* __restrict__ out, int64_t t0) {
     const int64_t total = M * N;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t t = k / M;
+        const int64_t t = t0 + k / M;
         const int64_t i = t / I;
         bool keep = i < nint;
         if (keep) keep = !exceed[i] && !exceed[i + 1] && !(i >= 1 && exceed[i - 1]);
@@ -106,12 +107,40 @@ int64_t mask_out_artifacts_device(const float* X, int64_t M, int64_t N, double t
         MS3_LAUNCH_CHECK();
     }
     const int64_t blocks = std::min<int64_t>(ceil_div(M * N, 256), (int64_t)sm_count() * 32);
-    artifact_write<<<(unsigned)blocks, 256, 0, stream>>>(X, M, N, I, nint, exceed.as<int>(), out);
+    artifact_write<<<(unsigned)blocks, 256, 0, stream>>>(X, M, N, I, nint, exceed.as<int>(), out, 0);
     MS3_LAUNCH_CHECK();
+    return artifact_kept(exceed.as<int>(), nint, I, stream);
+}
+
+void artifact_norms_device(const float* X, int64_t M, int64_t I, int64_t nint, double* norms, cudaStream_t stream) {
+    if (M <= 0 || nint <= 0) return;
+    if (nint > 0x7fffffff) throw_unsupported("too many intervals");
+    const int threads = 128;
+    const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(M, threads), 65535));
+    artifact_norms<<<dim3(gx, (unsigned)nint), threads, 0, stream>>>(X, M, I, nint, norms);
+    MS3_LAUNCH_CHECK();
+}
+
+void artifact_flags_device(const double* norms, int64_t M, int64_t nint, double threshold, int* exceed,
+                           cudaStream_t stream) {
+    MS3_CUDA(cudaMemsetAsync(exceed, 0, sizeof(int) * (size_t)(nint + 2), stream));
+    if (M <= 0 || nint <= 0) return;
+    artifact_flags<<<(unsigned)ceil_div(M, 128), 128, 0, stream>>>(norms, M, nint, threshold, exceed);
+    MS3_LAUNCH_CHECK();
+}
+
+void artifact_write_device(const float* X, int64_t M, int64_t rows, int64_t t0, int64_t I, int64_t nint,
+                           const int* exceed, float* out, cudaStream_t stream) {
+    if (M <= 0 || rows <= 0) return;
+    const int64_t blocks = std::min<int64_t>(ceil_div(M * rows, 256), (int64_t)sm_count() * 32);
+    artifact_write<<<(unsigned)blocks, 256, 0, stream>>>(X, M, rows, I, nint, exceed, out, t0);
+    MS3_LAUNCH_CHECK();
+}
+
+int64_t artifact_kept(const int* exceed, int64_t nint, int64_t I, cudaStream_t stream) {
     // timepoints kept, for the reference's "Using x% of all timepoints" line
     std::vector<int> h((size_t)(nint + 2));
-    MS3_CUDA(cudaMemcpyAsync(h.data(), exceed.get(), sizeof(int) * (size_t)(nint + 2), cudaMemcpyDeviceToHost,
-                             stream));
+    MS3_CUDA(cudaMemcpyAsync(h.data(), exceed, sizeof(int) * (size_t)(nint + 2), cudaMemcpyDeviceToHost, stream));
     MS3_CUDA(cudaStreamSynchronize(stream));
     int64_t kept = 0;
     for (int64_t i = 0; i < nint; i++)

@@ -856,6 +856,18 @@ int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dtype, const 
     });
 }
 
+int ms3gpu_mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int64_t interval_size,
+                                     const ms3gpu_stream_io* io, int64_t* timepoints_kept, void* stream) {
+    return guarded([&] {
+        check_shape(M, N);
+        if (threshold == 0 || interval_size <= 0)
+            throw_invalid("Problem with input parameters. Either threshold or interval_size is zero.");
+        check_stream_io(io, true);
+        const int64_t kept = mask_out_artifacts_stream(M, N, threshold, interval_size, *io, as_stream(stream));
+        if (timepoints_kept) *timepoints_kept = kept;
+    });
+}
+
 int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io, const ms3gpu_whiten_opts* opts,
                          void* stream) {
     return guarded([&] {

@@ -471,14 +471,17 @@ int run_mask_out_artifacts(const CLParams& clp) {
         return -1;
     }
     std::string err;
-    std::vector<float> X;
-    int64_t M = 0, N = 0;
-    if (!ms3io::read_timeseries_any_f32(in, M, N, X, err)) return fail(err);
-    std::vector<float> Y((size_t)(M * N));
+    // two passes over the input in blocks of whole intervals (the norms,
+    // then the masked copy), as the reference reads it twice
+    StreamFiles f;
+    if (!f.in.open(in, err)) return fail(err);
+    const int64_t M = f.in.M(), N = f.in.N();
+    if (!f.out.open(out, ms3io::kFloat32, M, N, err)) return fail(err);
+    const ms3gpu_stream_io io = stream_io(f, clp);
     int64_t kept = 0;
-    if (ms3gpu_mask_out_artifacts(X.data(), M, N, threshold, interval_size, Y.data(), &kept, nullptr) != MS3GPU_OK)
-        return fail(ms3gpu_last_error());
-    if (!ms3io::write_timeseries(out, ms3io::kFloat32, M, N, Y.data(), err)) return fail(err);
+    if (ms3gpu_mask_out_artifacts_stream(M, N, threshold, interval_size, &io, &kept, nullptr) != MS3GPU_OK)
+        return stream_fail(f);
+    if (!f.out.commit(err)) return fail(err);
     const int64_t nint = N / interval_size;
     if (nint > 0) std::printf("Using %.2f%% of all timepoints\n", kept * 100.0 / (double)(nint * interval_size));
     return 0;

@@ -1,4 +1,4 @@
-// Streaming forms of ms3.bandpass_filter and ms3.whiten.
+// Streaming forms of ms3.bandpass_filter, ms3.whiten and ms3.mask_out_artifacts.
 //
 // The reference reads its input in chunks through DiskReadMda32::readChunk
 // (mda/diskreadmda32.cpp:615-661) and writes them with
@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <string>
 
+#include "artifacts.h"
 #include "bandpass.h"
 #include "common.cuh"
 #include "ms3gpu.h"
@@ -253,6 +254,47 @@ void whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io& io, double quan
     MS3_CUDA(cudaMemcpyAsync(&herr, errbuf.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     MS3_CUDA(cudaStreamSynchronize(s));
     if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+}
+
+int64_t mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int64_t I, const ms3gpu_stream_io& io,
+                                  cudaStream_t s) {
+    if (M <= 0 || N <= 0) return 0;
+    const int64_t nint = N / I;
+    const size_t row_bytes = sizeof(float) * (size_t)M;
+    // slabs of whole intervals
+    const int64_t R = std::max<int64_t>(1, slab_bytes_of(io) / (int64_t)row_bytes / I) * I;
+    const int64_t rows_max = std::min(N, R);
+    SlabPipe pipe(row_bytes * (size_t)rows_max, row_bytes * (size_t)rows_max, s);
+    DevBuf norms(sizeof(double) * (size_t)std::max<int64_t>(1, nint * M), s);
+    DevBuf exceed(sizeof(int) * (size_t)(nint + 2), s);
+    // pass 1 (p_mask_out_artifacts.cpp:37-58): norms of the whole intervals,
+    // which end at timepoint nint * I
+    const int64_t covered = nint * I;
+    pipe.run(ceil_div(covered, R), row_bytes, 0, io,
+             [&](int64_t k) {
+                 SlabRows r;
+                 r.a = k * R;
+                 r.b = std::min(covered, (k + 1) * R);
+                 return r;
+             },
+             [&](int64_t, const SlabRows& r, void* din, void*) {
+                 artifact_norms_device(static_cast<const float*>(din), M, I, (r.b - r.a) / I,
+                                       norms.as<double>() + (r.a / I) * M, s);
+             });
+    artifact_flags_device(norms.as<double>(), M, nint, threshold, exceed.as<int>(), s);
+    // pass 2 (:60-99): the masked copy, zeros beyond the last whole interval
+    pipe.run(ceil_div(N, R), row_bytes, row_bytes, io,
+             [&](int64_t k) {
+                 SlabRows r;
+                 r.a = r.o0 = k * R;
+                 r.b = r.o1 = std::min(N, (k + 1) * R);
+                 return r;
+             },
+             [&](int64_t, const SlabRows& r, void* din, void* dout) {
+                 artifact_write_device(static_cast<const float*>(din), M, r.b - r.a, r.a, I, nint,
+                                       exceed.as<int>(), static_cast<float*>(dout), s);
+             });
+    return artifact_kept(exceed.as<int>(), nint, I, s);
 }
 
 }  // namespace ms3gpu

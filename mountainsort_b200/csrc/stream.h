@@ -23,4 +23,10 @@ void bandpass_stream(int64_t M, int64_t N, bool in_i16, const ms3gpu_stream_io& 
 void whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io& io, double quantization_unit, bool mixed,
                    cudaStream_t s);
 
+// ms3.mask_out_artifacts with two passes over the input (interval norms,
+// then the masked copy), slabs of whole intervals; identical values and
+// timepoints kept to the in-memory call.  Returns the timepoints kept.
+int64_t mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int64_t interval_size,
+                                  const ms3gpu_stream_io& io, cudaStream_t s);
+
 }  // namespace ms3gpu

@@ -100,6 +100,9 @@ def _io(read=True, write=True, slab_bytes=0):
     lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io()), None, None),
     lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io(write=False)), ctypes.byref(w), None),
     lambda L, o, w: L.ms3gpu_whiten_stream(4, 10, ctypes.byref(_io()), ctypes.byref(_lib.WhitenOpts(0, 7)), None),
+    lambda L, o, w: L.ms3gpu_mask_out_artifacts_stream(4, 10, 0.0, 2000, ctypes.byref(_io()), None, None),
+    lambda L, o, w: L.ms3gpu_mask_out_artifacts_stream(4, 10, 6.0, 0, ctypes.byref(_io()), None, None),
+    lambda L, o, w: L.ms3gpu_mask_out_artifacts_stream(4, 10, 6.0, 2000, ctypes.byref(_io(write=False)), None, None),
 ])
 def test_stream_arguments_rejected_before_device_work(make):
     """The streaming entry points check their callbacks, dtype, slab size,

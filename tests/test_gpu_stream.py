@@ -278,3 +278,35 @@ def test_executable_whitening_matrix_processors_in_blocks(gpu_lib, ref32, tmp_pa
              f"--timeseries_out={po}", "--quantization_unit=0.05", "--_slab_mb=1")
     assert r.returncode == 0, r.stderr
     np.testing.assert_array_equal(mdaio.readmda(po).T, api.apply_whitening_matrix(A, W, quantization_unit=0.05))
+
+
+@pytest.mark.parametrize("M,N,I,slab", [(32, 1_000_000, 2000, 1), (7, 300_123, 777, 5 * 777 * 7 * 4), (16, 1500, 2000, 1)])
+def test_mask_out_artifacts_stream_equals_in_memory(gpu_lib, M, N, I, slab):
+    X = api.bandpass_filter(synth.generate_numpy(M, N, K=2, seed=N % 97), FS, FMIN, FMAX, FWID,
+                            num_threads=max(16, 187 // M + 1))
+    rng = np.random.default_rng(5)
+    for t in rng.integers(0, max(1, N - 500), 6):  # artifacts to mask
+        X[t:t + 300, rng.integers(0, M)] += 5000.0
+    ref, kept_ref = api.mask_out_artifacts(X, 6.0, I, return_kept=True)
+    rec = Recorder(X, N, M, np.float32)
+    kept = api.mask_out_artifacts_stream(rec.source, rec.sink, M, N, 6.0, I, slab_bytes=slab)
+    assert kept == kept_ref
+    assert rec.written.all()
+    np.testing.assert_array_equal(rec.Y, ref)
+    # two passes: the norms read only whole intervals, then every timepoint
+    nint = N // I
+    assert sum(nt for t0, nt in rec.reads) == nint * I + N
+
+
+def test_executable_masks_in_blocks(gpu_lib, tmp_path):
+    M, N = 16, 400_000
+    X = api.bandpass_filter(synth.generate_numpy(M, N, K=3, seed=77), FS, FMIN, FMAX, FWID, num_threads=16)
+    X[123456:124000, 3] += 4000.0
+    pin, pout = str(tmp_path / "f.mda"), str(tmp_path / "m.mda")
+    mdaio.writemda(X.T, pin)
+    r = _run("ms3.mask_out_artifacts", f"--timeseries={pin}", f"--timeseries_out={pout}", "--threshold=6",
+             "--interval_size=2000", "--_slab_mb=1")
+    assert r.returncode == 0, r.stderr
+    ref, kept = api.mask_out_artifacts(X, 6.0, 2000, return_kept=True)
+    np.testing.assert_array_equal(mdaio.readmda(pout).T, ref)
+    assert f"Using {kept * 100.0 / (N // 2000 * 2000):.2f}% of all timepoints" in r.stdout
