@@ -49,6 +49,12 @@ SPEC = {
         "outputs": ["timeseries_out"],
         "parameters": [("quantization_unit", True, 0)],
     },
+    "ms3.mask_out_artifacts": {
+        "version": "0.1",
+        "inputs": ["timeseries"],
+        "outputs": ["timeseries_out"],
+        "parameters": [("threshold", True, 6), ("interval_size", True, 2000)],
+    },
 }
 
 
@@ -159,6 +165,27 @@ def whiten_clips(clips, whitening_matrix, clips_out, quantization_unit=0) -> boo
 PROCESSORS = {"ms3.bandpass_filter": bandpass_filter, "ms3.whiten": whiten,
               "ms3.compute_whitening_matrix": compute_whitening_matrix,
               "ms3.apply_whitening_matrix": apply_whitening_matrix, "ms3.whiten_clips": whiten_clips}
+
+
+def mask_out_artifacts(timeseries, timeseries_out, threshold=6, interval_size=2000) -> bool:
+    """ms3.mask_out_artifacts (p_mask_out_artifacts.cpp:24-104), streaming the
+    memory-mapped input twice (interval norms, then the masked copy).
+    Returns False, like the reference, when threshold or interval_size is 0."""
+    threshold, interval_size = float(threshold), int(interval_size)
+    if threshold == 0 or interval_size <= 0:
+        return False
+    M, N, rows = mdaio.timeseries_rows_view(timeseries)
+    out = mdaio.TimeseriesWriter(timeseries_out, np.float32, M, N)
+    try:
+        api.mask_out_artifacts_stream(lambda t0, nt: rows[t0:t0 + nt], out.write, M, N, threshold, interval_size)
+    except BaseException:
+        out.abort()
+        raise
+    out.close()
+    return True
+
+
+PROCESSORS["ms3.mask_out_artifacts"] = mask_out_artifacts
 
 
 def run(name: str, **kwargs) -> bool:

@@ -161,3 +161,26 @@ def test_mask_out_artifacts_spec_and_parameter_check(tmp_path):
     out = str(tmp_path / "o.mda")
     r = run("ms3.mask_out_artifacts", f"--timeseries={p}", f"--timeseries_out={out}", "--threshold=0")
     assert r.returncode == 255 and "zero" in r.stdout and not os.path.exists(out)
+
+
+def test_python_processor_mirror_matches_the_executable_spec(tmp_path):
+    # processors.py mirrors every processor of ms3gpu.mp with the same
+    # version, inputs, outputs and parameter defaults
+    from mountainsort_b200 import processors
+
+    exe = {p["name"]: p for p in json.loads(run("spec").stdout)["processors"]}
+    assert set(processors.SPEC) == set(exe) == set(processors.PROCESSORS)
+    for name, spec in processors.SPEC.items():
+        e = exe[name]
+        assert spec["version"] == e["version"], name
+        assert spec["inputs"] == [i["name"] for i in e["inputs"]], name
+        assert spec["outputs"] == [o["name"] for o in e["outputs"]], name
+        for pname, optional, default in spec["parameters"]:
+            ep = {p["name"]: p for p in e["parameters"]}[pname]
+            assert ep["optional"] == optional, (name, pname)
+            if default is not None:
+                assert ep["default_value"] == default, (name, pname)
+    # zero threshold / interval are refused before any file is touched
+    out = str(tmp_path / "o.mda")
+    assert processors.run("ms3.mask_out_artifacts", timeseries="missing.mda", timeseries_out=out, threshold=0) is False
+    assert not os.path.exists(out)

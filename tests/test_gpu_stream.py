@@ -310,3 +310,16 @@ def test_executable_masks_in_blocks(gpu_lib, tmp_path):
     ref, kept = api.mask_out_artifacts(X, 6.0, 2000, return_kept=True)
     np.testing.assert_array_equal(mdaio.readmda(pout).T, ref)
     assert f"Using {kept * 100.0 / (N // 2000 * 2000):.2f}% of all timepoints" in r.stdout
+
+
+def test_python_mask_processor_streams_files(gpu_lib, tmp_path):
+    from mountainsort_b200 import processors
+
+    M, N = 8, 120_000
+    X = api.bandpass_filter(synth.generate_numpy(M, N, K=2, seed=3), FS, FMIN, FMAX, FWID, num_threads=24)
+    X[50000:50400, 2] += 3000.0
+    pin, pout = str(tmp_path / "f.mda"), str(tmp_path / "m.mda")
+    mdaio.writemda(X.T, pin)
+    assert processors.run("ms3.mask_out_artifacts", timeseries=pin, timeseries_out=pout, threshold=6,
+                          interval_size=1000)
+    np.testing.assert_array_equal(mdaio.readmda(pout).T, api.mask_out_artifacts(X, 6.0, 1000))
