@@ -176,14 +176,19 @@ MS3GPU_API int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int6
  * array that is part of the library's device image (every GPU that loads the
  * library holds it until the process exits); it allocates nothing.
  *
- * timeseries and XXt must be device memory of the current device (host
- * buffers would need staging, which allocates); other pointers are rejected
- * with MS3GPU_ERR_INVALID, and so is M above 1984 channels, the most whose
- * 64 x 64 partial tiles fit the array.  The first call on a device looks the
- * array's device address up (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the one array, so calls that
- * overlap on the GPU (other streams, other host threads) race: serialise
- * them.  Each call overwrites every part of the array it reads. */
+ * timeseries and XXt must be device memory of the current device or managed
+ * memory (host buffers would need staging, which allocates); other pointers
+ * are rejected with MS3GPU_ERR_INVALID, and so is M above 1984 channels, the
+ * most whose 64 x 64 partial tiles fit the array.  The work is queued on
+ * `stream` and the call returns without waiting for it: XXt is ready once
+ * the stream reaches that point (synchronise the stream, or order later work
+ * after it).  The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not keep using the entry
+ * point after cudaDeviceReset on that device (the kept address would be
+ * stale).  All calls share the one array, so calls that overlap on the GPU
+ * (other streams, other host threads) race: serialise them.  Each call
+ * overwrites every part of the array it reads. */
 MS3GPU_API int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t N, double* XXt,
                                                 void* stream);
 

@@ -27,18 +27,21 @@ namespace ms3gpu {
 
 namespace {
 
-// norms[i * M + m]; threads over channels, blocks over intervals
+// norms[i * M + m]; threads over channels, blocks over intervals (the grid's
+// y extent is capped at 65535, so each block row strides over the intervals)
 __global__ void artifact_norms(const float* __restrict__ X, int64_t M, int64_t I, int64_t nint,
                                double* __restrict__ norms) {
-    const int64_t i = blockIdx.y;
-    for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < M; m += (int64_t)gridDim.x * blockDim.x) {
-        const float* p = X + i * I * M + m;
-        double s = 0.0;
-        for (int64_t a = 0; a < I; a++) {
-            const double v = (double)p[a * M];
-            s = __dadd_rn(s, __dmul_rn(v, v));
+    for (int64_t i = blockIdx.y; i < nint; i += gridDim.y) {
+        for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < M;
+             m += (int64_t)gridDim.x * blockDim.x) {
+            const float* p = X + i * I * M + m;
+            double s = 0.0;
+            for (int64_t a = 0; a < I; a++) {
+                const double v = (double)p[a * M];
+                s = __dadd_rn(s, __dmul_rn(v, v));
+            }
+            norms[i * M + m] = sqrt(s);
         }
-        norms[i * M + m] = sqrt(s);
     }
 }
 
@@ -97,11 +100,7 @@ int64_t mask_out_artifacts_device(const float* X, int64_t M, int64_t N, double t
     DevBuf exceed(sizeof(int) * (size_t)(nint + 2), stream);
     MS3_CUDA(cudaMemsetAsync(exceed.get(), 0, sizeof(int) * (size_t)(nint + 2), stream));
     if (nint > 0) {
-        if (nint > 0x7fffffff) throw_unsupported("too many intervals");
-        const int threads = 128;
-        const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(M, threads), 65535));
-        artifact_norms<<<dim3(gx, (unsigned)nint), threads, 0, stream>>>(X, M, I, nint, norms.as<double>());
-        MS3_LAUNCH_CHECK();
+        artifact_norms_device(X, M, I, nint, norms.as<double>(), stream);
         artifact_flags<<<(unsigned)ceil_div(M, 128), 128, 0, stream>>>(norms.as<double>(), M, nint, threshold,
                                                                       exceed.as<int>());
         MS3_LAUNCH_CHECK();
@@ -114,10 +113,10 @@ int64_t mask_out_artifacts_device(const float* X, int64_t M, int64_t N, double t
 
 void artifact_norms_device(const float* X, int64_t M, int64_t I, int64_t nint, double* norms, cudaStream_t stream) {
     if (M <= 0 || nint <= 0) return;
-    if (nint > 0x7fffffff) throw_unsupported("too many intervals");
     const int threads = 128;
     const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(M, threads), 65535));
-    artifact_norms<<<dim3(gx, (unsigned)nint), threads, 0, stream>>>(X, M, I, nint, norms);
+    const unsigned gy = (unsigned)std::min<int64_t>(nint, 65535);
+    artifact_norms<<<dim3(gx, gy), threads, 0, stream>>>(X, M, I, nint, norms);
     MS3_LAUNCH_CHECK();
 }
 

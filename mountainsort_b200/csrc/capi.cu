@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "ms3gpu.h"
 #include "pipeline.h"
+#include "ptrkind.h"
 #include "stream.h"
 #include "whiten.h"
 
@@ -93,6 +94,10 @@ void DevBuf::release() {
 
 namespace {
 
+// True for memory the current device reaches in place (its own device
+// memory, managed memory), false for host memory, which is staged.  Device
+// memory of another GPU is rejected: a kernel given it would fault rather
+// than fail cleanly.
 bool is_device_ptr(const void* p) {
     if (!p) return false;
     cudaPointerAttributes a;
@@ -100,7 +105,18 @@ bool is_device_ptr(const void* p) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    int cur = 0;
+    MS3_CUDA(cudaGetDevice(&cur));
+    switch (classify_pointer((int)a.type, a.device, cur)) {
+    case PtrKind::DeviceHere:
+    case PtrKind::Managed:
+        return true;
+    case PtrKind::DeviceElsewhere:
+        throw_invalid("buffer is device memory of GPU " + std::to_string(a.device) + ", but the call runs on GPU " +
+                      std::to_string(cur) + " (make that device current or copy the buffer)");
+    default:
+        return false;
+    }
 }
 
 // A read-only view of a caller buffer on the device.
@@ -433,12 +449,13 @@ int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t
         cudaStream_t s = as_stream(stream);
         require(timeseries, "timeseries", M * N > 0);
         require(XXt, "XXt", M > 0);
-        // Staging host memory would allocate device buffers: only device memory is accepted.
+        // Staging host memory would allocate device buffers: only memory the
+        // current device reaches in place is accepted.
         if (M * N > 0 && !is_device_ptr(timeseries))
             throw_invalid("ms3gpu_whiten_covariance_noalloc needs timeseries in device memory");
         if (M > 0 && !is_device_ptr(XXt)) throw_invalid("ms3gpu_whiten_covariance_noalloc needs XXt in device memory");
+        // Queued on the caller's stream; the caller decides when to wait for it.
         covariance_device_noalloc(timeseries, M, N, XXt, s);
-        MS3_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -2,7 +2,7 @@
 
 Run in a checkout where the reference project is available:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <root of the reference checkout>
 
 1. .mda files written by the reference's own Python writer
    (packages/pyms/mlpy/mdaio.py: writemda8/16i/16ui/32/32i/32ui/64 and
@@ -100,7 +100,9 @@ def make_oracle_fixtures():
 
 
 if __name__ == "__main__":
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <root of the reference checkout>")
+    ref_root = sys.argv[1]
     make_mda_fixtures(ref_root)
     make_oracle_fixtures()
     print("fixtures written to", HERE)

@@ -57,3 +57,25 @@ def test_mask_out_artifacts_processor(gpu_lib, ref32, tmp_path):
     assert "Using" in r.stdout and "of all timepoints" in r.stdout
     ref, _ = ref32.mask_out_artifacts(X, threshold=5, interval_size=1500)
     np.testing.assert_array_equal(mdaio.readmda(o).T, ref)
+
+
+def test_mask_out_artifacts_more_intervals_than_a_grid_row(gpu_lib, ref32):
+    """More than 65535 intervals (the largest grid y extent): the norm kernel
+    strides over them, in memory and in one streamed slab."""
+    M, N, I = 1, 140_001, 2  # 70000 intervals
+    X = _with_artifacts(M, N, seed=11)
+    ref, kept_ref = ref32.mask_out_artifacts(X, threshold=4.0, interval_size=I)
+    got, kept = api.mask_out_artifacts(X, threshold=4.0, interval_size=I, return_kept=True)
+    np.testing.assert_array_equal(got, ref)
+    assert kept == kept_ref and 0 < kept < (N // I) * I
+    Y = np.full_like(X, 7.0)
+
+    def source(t0, nt):
+        return X[t0:t0 + nt]
+
+    def sink(t0, rows):
+        Y[t0:t0 + len(rows)] = rows
+
+    kept_s = api.mask_out_artifacts_stream(source, sink, M, N, 4.0, I)
+    assert kept_s == kept_ref
+    np.testing.assert_array_equal(Y, ref)

@@ -1,0 +1,94 @@
+"""The whole bandpass_filter -> whiten chain through the C ABI against the
+oracle at the benchmark's channel counts and lengths.
+
+  * 384 channels x 600,000 timepoints (20 s at 30 kHz, the profiling case of
+    the 384-channel benchmark): filtered and whitened outputs vs ref32, each
+    relative L2 <= 1e-5 (plain FP32 form).
+  * 32 channels x 1,800,000 timepoints (60 s, the CPU-sized configuration):
+    plain form vs ref32 <= 1e-5; the mixed-precision form vs the FP64 oracle
+    <= 1e-4.
+  * 4 shanks x 384 channels (1536 in all), int16 input with the amplifier
+    gain 0.195 folded into the integers, 300,000 timepoints, each shank
+    whitened on its own: plain form vs ref32 per shank <= 1e-5; mixed form vs
+    the FP64 oracle <= 1e-4.
+
+ref32 whitens the filtered signal ref32 produced, so each comparison covers
+the complete chain.  The errors are printed (pytest -s shows them) with the
+largest absolute difference.
+"""
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from mountainsort_b200 import api, synth
+from oracle import oracle64 as o64
+
+pytestmark = pytest.mark.gpu
+
+FS, FMIN, FMAX, FWID = 30000.0, 300.0, 6000.0, 1000.0
+
+
+def _report(what, got, ref):
+    e = o64.rel_l2(got, ref)
+    mx = float(np.max(np.abs(np.asarray(got, np.float64) - np.asarray(ref, np.float64))))
+    print(f"{what}: rel L2 {e:.3e}, max-abs {mx:.3e}")
+    return e
+
+
+def _recording(M, N, K, seed):
+    return synth.generate_torch(M, N, K=K, seed=seed, sites=(6, 12)).cpu().numpy()
+
+
+def test_chain_384ch_600k_vs_ref32(gpu_lib, ref32):
+    X = _recording(384, 600_000, 40, seed=2)
+    filt, pre = api.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=16, want_filt=True)
+    filt_ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre_ref, _, _ = ref32.whiten(filt_ref)
+    assert _report("384x600k filt vs ref32", filt, filt_ref) <= 1e-5
+    assert _report("384x600k pre vs ref32", pre, pre_ref) <= 1e-5
+
+
+def test_chain_32ch_60s_plain_and_mixed(gpu_lib, ref32):
+    X = synth.generate_numpy(32, 1_800_000, K=20, seed=0, sites=(3, 6))
+    filt, pre = api.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=16, want_filt=True)
+    filt_ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre_ref, _, _ = ref32.whiten(filt_ref)
+    assert _report("32x1.8M filt vs ref32", filt, filt_ref) <= 1e-5
+    assert _report("32x1.8M pre vs ref32", pre, pre_ref) <= 1e-5
+    mixed = api.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=16, precision="mixed")
+    f64 = o64.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    _, q64, _, _ = o64.whiten(f64)
+    assert _report("32x1.8M mixed pre vs FP64 oracle", mixed, q64) <= 1e-4
+    _report("32x1.8M plain pre vs FP64 oracle", pre, q64)
+    _report("32x1.8M ref32 pre vs FP64 oracle (the FP32 floor)", pre_ref, q64)
+
+
+def test_chain_4_shanks_of_384_int16(gpu_lib, ref32):
+    M1, N = 384, 300_000
+    X = np.hstack([_recording(M1, N, 300, seed=100 + k) for k in range(4)])
+    X16 = np.clip(np.round(X / 0.195), -32768, 32767).astype(np.int16)
+    del X
+    shanks = [list(range(1 + M1 * k, 1 + M1 * (k + 1))) for k in range(4)]
+    filt = api.bandpass_filter(X16, FS, FMIN, FMAX, FWID, num_threads=16)
+    pre = api.whiten_blocks(filt, shanks)
+    mixed = api.whiten_blocks(filt, shanks, precision="mixed")
+    # the reference reads int16 and converts each value to float
+    filt_ref = ref32.bandpass_filter(X16.astype(np.float32), FS, FMIN, FMAX, FWID, num_threads=16)
+    assert _report("4x384 int16 filt vs ref32", filt, filt_ref) <= 1e-5
+
+    def shank_ref(k):
+        cols = slice(M1 * k, M1 * (k + 1))
+        return ref32.whiten(np.ascontiguousarray(filt_ref[:, cols]))[0]
+
+    with ThreadPoolExecutor(4) as ex:  # the oracle's calls release the GIL
+        refs = list(ex.map(shank_ref, range(4)))
+    for k in range(4):
+        cols = slice(M1 * k, M1 * (k + 1))
+        assert _report(f"4x384 int16 shank {k} pre vs ref32", pre[:, cols], refs[k]) <= 1e-5
+    f64 = o64.bandpass_filter(X16.astype(np.float32), FS, FMIN, FMAX, FWID, num_threads=16)
+    q64 = np.empty(mixed.shape, np.float64)
+    for k in range(4):
+        cols = slice(M1 * k, M1 * (k + 1))
+        q64[:, cols] = o64.whiten(np.ascontiguousarray(f64[:, cols]))[1]
+    assert _report("4x384 int16 mixed pre vs FP64 oracle", mixed, q64) <= 1e-4

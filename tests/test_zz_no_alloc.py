@@ -5,11 +5,13 @@ This entry point is for callers that cannot let the library call cudaMalloc
 processing starts, and streaming loops that must not stall on a device
 allocation.  It keeps its partial sums in a fixed 16 MiB array inside the
 library's device image.  These tests call it through the C ABI with device
-buffers and compare it with the allocating entry point
-(ms3gpu_whiten_covariance), on two calls in a row, within the covariance
-tolerance the other tests use (1e-12 relative: the two differ only in the
-order of FP64 partial sums).  The file sorts last so that a run stopping at
-its first failure has already run every other test.
+buffers and compare it, on two calls in a row, with the allocating entry
+point (ms3gpu_whiten_covariance; 1e-12 relative, the two differ only in the
+order of FP64 partial sums) and with the oracle's covariance pass on the same
+input (1e-8 relative, the covariance tolerance of the other tests).  The call
+only queues its work on the stream, so the tests read the result after the
+stream has reached it.  The file sorts last so that a run stopping at its
+first failure has already run every other test.
 """
 import ctypes
 
@@ -28,19 +30,23 @@ def _noalloc(L, X, out, stream):
 
 
 @pytest.mark.parametrize("M,N", [(64, 200000), (384, 60000)])
-def test_noalloc_covariance_matches_allocating_entry_point(gpu_lib, M, N):
+def test_noalloc_covariance_matches_allocating_entry_point(gpu_lib, ref32, M, N):
     import torch
 
     L = gpu_lib
-    X = torch.from_numpy(synth.generate_numpy(M, N, K=4, seed=M)).cuda()
+    Xh = synth.generate_numpy(M, N, K=4, seed=M)
+    X = torch.from_numpy(Xh).cuda()
     ref = api.whiten_covariance(X).cpu().numpy()  # allocating entry point, matrix notation
+    oracle = ref32.whiten_xxt(Xh)  # the oracle's pass 1 (float products summed in double)
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(2):  # the second call runs on the array the first one left behind
         out = torch.full((M, M), float("nan"), dtype=torch.float64, device="cuda")
         assert _noalloc(L, X, out, stream) == _lib.OK, _lib.last_error()
+        torch.cuda.current_stream().synchronize()  # the call returns before its work is done
         got = out.cpu().numpy().T  # column-major buffer -> matrix notation
         assert np.all(np.isfinite(got))
         assert o64.rel_l2(got, ref) <= 1e-12
+        assert o64.rel_l2(got, oracle) <= 1e-8
         np.testing.assert_array_equal(got, got.T)
 
 
