@@ -24,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -104,52 +105,162 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- CPU baseline
 
+class CpuReference:
+    """The reference's CPU path timed on this host's cores.
+
+    Where oracle/_ref/libmsref.so exists (the reference's own
+    packages/ms3/p_bandpass_filter.cpp, p_whiten.cpp and pca.cpp compiled from
+    its sources; its FFT interface runs the oracle's FFT), the bandpass
+    processor and the whitening matrix run that code; otherwise ref32, the
+    restatement that reproduces it bit for bit.  The whitening loops (pass 1
+    XX^T and pass 2 apply, p_whiten.cpp:75-113,153-206) run ref32's copy of
+    them, one slice per thread on every thread at once, as the reference's
+    OpenMP loop gives each thread its own chunk.
+
+    A full 384 x 18M recording takes the reference about 15 minutes on 16
+    cores (the apply alone is ~0.7 ms per timepoint per thread), so one
+    measured sample is:
+      * bandpass: one parallel round of the reference geometry (T chunks of
+        `chunk` timepoints, one per thread), file to file through the
+        processor (page-cache I/O included, as the reference runs);
+      * whiten loops: T threads x `wh_rows` timepoints each, pass 1 and pass 2;
+      * the whitening matrix at the real M, once per process (O(M^4), serial).
+    The recording's time is then rounds x each part + the matrix; the value is
+    M*N / that time.  ms_per_step is the wall time of one measured sample."""
+
+    def __init__(self, M, N, threads, wh_rows=6250):
+        import numpy as np
+
+        from oracle import ref32, refpin
+
+        self.np, self.ref32, self.refpin = np, ref32, refpin
+        self.M, self.N, self.T = M, N, max(1, threads)
+        self.kind = "reference" if refpin.available() else "port"
+        self.chunk = ref32.chunk_size(M, GEOM_T)
+        self.wh_rows = wh_rows
+        rng = np.random.default_rng(1)
+        # one parallel round of the bandpass geometry, written once as the processor's input file
+        self.tmp = tempfile.mkdtemp(prefix="ms3ref_")
+        rows = self.T * self.chunk
+        X = (10 * rng.standard_normal((rows, M))).astype(np.float32)
+        self.bp_in = os.path.join(self.tmp, "raw.mda")
+        from mountainsort_b200 import mdaio
+
+        mdaio.writemda(X.T, self.bp_in)
+        self.wh = [np.ascontiguousarray(X[k * wh_rows:(k + 1) * wh_rows]) for k in range(self.T)]
+        del X
+        # the whitening matrix at the real channel count (serial O(M^4) power iteration)
+        C = np.cov(rng.standard_normal((M, 4 * M))) + np.eye(M)
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            refpin.whitening_matrix(C)
+        else:
+            ref32.whitening_matrix(C)
+        self.t_W = time.perf_counter() - t0
+        self.samples = []
+
+    def sample(self):
+        from concurrent.futures import ThreadPoolExecutor
+
+        np, ref32, refpin = self.np, self.ref32, self.refpin
+        t0 = time.perf_counter()
+        out = os.path.join(self.tmp, "filt.mda")
+        if os.path.exists(out):
+            os.remove(out)
+        if self.kind == "reference":
+            if refpin.lib().msref_bandpass_filter(self.bp_in.encode(), out.encode(), FS, FMIN, FMAX, FWID, 0.0, 1,
+                                                  GEOM_T) != 0:
+                raise RuntimeError("reference bandpass processor failed")
+        else:
+            from mountainsort_b200 import mdaio
+
+            X = np.ascontiguousarray(mdaio.readmda(self.bp_in).T)
+            mdaio.writemda(ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=GEOM_T,
+                                                 exec_threads=self.T).T, out)
+        t_bp = time.perf_counter() - t0
+        W = np.eye(self.M)
+        t1 = time.perf_counter()
+        with ThreadPoolExecutor(self.T) as ex:  # the ctypes calls release the GIL
+            list(ex.map(lambda Y: ref32.whiten_xxt(Y, exec_threads=1), self.wh))
+        t_xxt = time.perf_counter() - t1
+        t2 = time.perf_counter()
+        with ThreadPoolExecutor(self.T) as ex:
+            list(ex.map(lambda Y: ref32.whiten_apply(Y, W, exec_threads=1), self.wh))
+        t_apply = time.perf_counter() - t2
+        rec = {"bp": t_bp, "xxt": t_xxt, "apply": t_apply, "wall": time.perf_counter() - t0}
+        self.samples.append(rec)
+        return rec
+
+    def total_seconds(self, rec):
+        rounds = -(-self.N // (self.T * self.chunk))
+        # the whitening loops run on 100000-timepoint chunks, one per thread per round
+        wrounds = -(-self.N // (self.T * 100000)) * (100000 / self.wh_rows)
+        return rounds * rec["bp"] + wrounds * (rec["xxt"] + rec["apply"]) + self.t_W
+
+    def describe(self, rec):
+        src = ("the reference's own processor code (oracle/_ref) for the bandpass and the whitening matrix"
+               if self.kind == "reference" else "ref32 (the bit-identical restatement)")
+        return (f"{src}; {self.T} threads on this host: bandpass processor file to file on one parallel round "
+                f"({self.T} chunks of {self.chunk} x {self.M}ch, {rec['bp']:.2f} s); whiten pass 1 / pass 2 loops "
+                f"on {self.T} x {self.wh_rows} timepoints at once ({rec['xxt']:.2f} s / {rec['apply']:.2f} s; "
+                f"{len(self.samples) * self.T * self.wh_rows} timepoints measured in all); whitening matrix at "
+                f"M={self.M}: {self.t_W:.1f} s once; recording time {self.total_seconds(rec):.1f} s for "
+                f"{self.M}x{self.N} = rounds x measured parts + matrix")
+
+    def close(self):
+        import shutil
+
+        shutil.rmtree(self.tmp, ignore_errors=True)
+
+
+def cpu_threads():
+    return max(1, int(os.environ.get("MS3_BENCH_CPU_THREADS", str(os.cpu_count() or 1))))
+
+
 def cpu_baseline(M: int, N: int, threads: int):
-    """Times the CPU restatement of the reference (oracle/ref32, OpenMP, the
-    reference's loop structure) on a bounded sample and models the full
-    recording from it.  Returns a cpu_baseline dict (value in Gch-samples/s)."""
+    """One measured sample of the CPU reference (see CpuReference)."""
+    ref = CpuReference(M, N, threads)
+    try:
+        rec = ref.sample()
+        total = ref.total_seconds(rec)
+        return {"value": M * N / total / 1e9, "unit": UNIT, "cores": ref.T, "kind": ref.kind,
+                "sample": ref.describe(rec)}
+    finally:
+        ref.close()
+
+
+def reference_c1_full(threads):
+    """Configuration 1 (32 x 1.8M, 60 s at 30 kHz) run in full through the
+    reference's own processors, file to file: bandpass then whiten."""
     import numpy as np
 
-    from oracle import ref32
+    from mountainsort_b200 import mdaio, synth
+    from oracle import refpin
 
-    rng = np.random.default_rng(1)
-    chunk = ref32.chunk_size(M, GEOM_T)
-    T = max(1, threads)
-    # bandpass: T chunks in parallel, one per thread (the reference's omp for)
-    Xs = (10 * rng.standard_normal((T * chunk, M))).astype(np.float32)
-    t0 = time.perf_counter()
-    ref32.bandpass_filter(Xs, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, exec_threads=T)
-    t_bp_round = time.perf_counter() - t0
-    del Xs
-    # whiten passes: per-timepoint cost of each pass on a 2000-timepoint slice (one thread)
-    S = 2000
-    Y = (rng.standard_normal((S, M))).astype(np.float32)
-    t0 = time.perf_counter()
-    C = ref32.whiten_xxt(Y, exec_threads=1)
-    t_xxt = (time.perf_counter() - t0) / S
-    W = np.eye(M)
-    t0 = time.perf_counter()
-    ref32.whiten_apply(Y, W, exec_threads=1)
-    t_apply = (time.perf_counter() - t0) / S
-    # power-iteration matrix: serial O(M^4); timed at M/2 and scaled by 16 for M > 256
-    Mp = M if M <= 256 else M // 2
-    C = np.cov(rng.standard_normal((Mp, 4 * Mp)))
-    t0 = time.perf_counter()
-    ref32.whitening_matrix(C)
-    t_pca = (time.perf_counter() - t0) * (M / Mp) ** 4
-    nchunks = -(-N // chunk)
-    wchunks = -(-N // 100000)
-    rounds = -(-nchunks // T)
-    wrounds = -(-wchunks // T)
-    total = rounds * t_bp_round + wrounds * 100000 * (t_xxt + t_apply) + t_pca
-    value = M * N / total / 1e9
-    return {
-        "value": value, "unit": UNIT, "cores": T, "kind": "port",
-        "sample": (f"ref32 (C++ restatement, OpenMP) on this host: {T} bandpass chunks of {chunk} x {M}ch in "
-                   f"parallel ({t_bp_round:.2f} s), whiten XXt/apply loops on {S} timepoints x {M}ch "
-                   f"({t_xxt * S:.2f} s / {t_apply * S:.2f} s, 1 thread), power-iteration W at M={Mp}"
-                   f"{' scaled x16' if Mp != M else ''}; modelled full run {total:.1f} s for {M}x{N}"),
-    }
+    if not refpin.available():
+        return None
+    M, N = 32, 1_800_000
+    X = synth.generate_numpy(M, N, K=20, seed=0, sites=(3, 6))
+    tmp = tempfile.mkdtemp(prefix="ms3ref_c1_")
+    try:
+        pin, pf, pp = (os.path.join(tmp, n) for n in ("raw.mda", "filt.mda", "pre.mda"))
+        mdaio.writemda(X.T, pin)
+        L = refpin.lib()
+        t0 = time.perf_counter()
+        if L.msref_bandpass_filter(pin.encode(), pf.encode(), FS, FMIN, FMAX, FWID, 0.0, 1, GEOM_T) != 0:
+            return None
+        t1 = time.perf_counter()
+        if L.msref_whiten(pf.encode(), pp.encode(), 0.0, threads) != 0:
+            return None
+        t2 = time.perf_counter()
+        return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1, timed in full",
+                "value": M * N / (t2 - t0) / 1e9, "unit": UNIT, "seconds": t2 - t0,
+                "bandpass_s": t1 - t0, "whiten_s": t2 - t1, "kind": "reference", "cores": threads,
+                "geometry_threads": GEOM_T}
+    finally:
+        import shutil
+
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def run_reference_arm(args, size):
@@ -157,22 +268,32 @@ def run_reference_arm(args, size):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    threads = min(threads, int(os.environ.get("MS3_BENCH_CPU_THREADS", "16")))
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(M, N, threads)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+    threads = cpu_threads()
+    t_start = time.perf_counter()
+    c1 = reference_c1_full(threads)
+    ref = CpuReference(M, N, threads)
+    try:
+        vals, walls = [], []
+        for i in range(args.warmup + args.steps):
+            rec = ref.sample()
+            if i >= args.warmup:
+                vals.append(M * N / ref.total_seconds(rec) / 1e9)
+                walls.append(rec["wall"])
+        v = statistics.median(vals)
+        cb = {"value": v, "unit": UNIT, "cores": ref.T, "kind": ref.kind, "sample": ref.describe(rec)}
+    finally:
+        ref.close()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": M * N / (v * 1e9) * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(walls) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": desc, "M": M, "N": N, "geometry_threads": GEOM_T, "freq": [FMIN, FMAX, FWID]},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timing": ("ms_per_step is the wall time of one measured sample (see cpu_baseline.sample); value is "
+                   "the recording's throughput from those measurements"),
+        "config1_full": c1,
+        "wall_s": time.perf_counter() - t_start,
     }
     print(json.dumps(line), flush=True)
 
@@ -347,8 +468,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = min(os.cpu_count() or 1, int(os.environ.get("MS3_BENCH_CPU_THREADS", "16")))
-        cpu = cpu_baseline(M, N, threads)
+        cpu = cpu_baseline(M, N, cpu_threads())
 
     if rank == 0:
         line = {
