@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libms3gpu.so")
 EXE = os.path.join(HERE, "ms3gpu.mp")
 
-CU_SOURCES = ["capi.cu", "bandpass.cu", "whiten.cu", "apply_tc.cu", "pipeline.cu", "stream.cu", "artifacts.cu", "detect.cu"]
+CU_SOURCES = ["capi.cu", "bandpass.cu", "whiten.cu", "apply_tc.cu", "pipeline.cu", "stream.cu", "artifacts.cu", "detect.cu", "cov_i8.cu"]
 EXE_SOURCES = ["ms3gpu_main.cpp", "mdaio.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -416,6 +416,7 @@ int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream)
         }
         MS3_CUDA(cudaEventDestroy(start));
         bandpass_check_timeout(s0);
+        covariance_check_timeout(s0);
     });
     if (rc != MS3GPU_OK) return rc;
     if (first_code != MS3GPU_OK) {
@@ -439,6 +440,7 @@ int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, doub
         covariance_device(static_cast<const float*>(in.ptr), M, N, static_cast<double*>(out.ptr), s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        covariance_check_timeout(s);
     });
 }
 
@@ -567,6 +569,7 @@ int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const i
         whitening_matrix_device(xxt.as<double>(), M2, static_cast<double*>(w.ptr), nullptr, nullptr, s);
         w.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        covariance_check_timeout(s);
     });
 }
 
@@ -627,6 +630,7 @@ int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const in
         int herr = 0;
         MS3_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         MS3_CUDA(cudaStreamSynchronize(s));
+        covariance_check_timeout(s);
         if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
     });
 }
@@ -730,6 +734,7 @@ int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeserie
                                out.ptr, s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        covariance_check_timeout(s);
     });
 }
 
@@ -780,6 +785,7 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         pre.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
         bandpass_check_timeout(s);
+        covariance_check_timeout(s);
     });
 }
 
@@ -849,6 +855,7 @@ int ms3gpu_whiten_covariance_sum(const float* timeseries, int64_t M, int64_t N, 
             covariance_sum_device(static_cast<const float*>(in.ptr), M, N, static_cast<double*>(out.ptr), s);
         out.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        covariance_check_timeout(s);
     });
 }
 

@@ -165,6 +165,7 @@ void bandpass_whiten_streamed(const float* raw_h, int64_t M, int64_t N, float* f
     MS3_CUDA(cudaStreamSynchronize(s));
     if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
     bandpass_check_timeout(s);
+    covariance_check_timeout(s);
 }
 
 }  // namespace ms3gpu

@@ -253,6 +253,7 @@ void whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io& io, double quan
     int herr = 0;
     MS3_CUDA(cudaMemcpyAsync(&herr, errbuf.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     MS3_CUDA(cudaStreamSynchronize(s));
+    covariance_check_timeout(s);
     if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
 }
 

@@ -632,15 +632,32 @@ int num_sms() {
 
 }  // namespace
 
+// MS3GPU_COV_KERNEL=fma keeps the FP32-FMA kernel for every shape; =tc uses
+// the tensor-core kernel whenever M % 4 == 0 (testing).  By default the
+// tensor cores take M >= 128 with M % 4 == 0.
+static int cov_kernel_choice() {
+    static const int v = [] {
+        const char* s = std::getenv("MS3GPU_COV_KERNEL");
+        if (s && std::string(s) == "fma") return 1;
+        if (s && std::string(s) == "tc") return 2;
+        return 0;
+    }();
+    return v;
+}
+
 CovPlan cov_plan(const float* X, int64_t M) {
     CovPlan p;
+    p.M = M;
     p.nb = (int)ceil_div(M, kCT);
     p.npairs = p.nb * (p.nb + 1) / 2;
     p.vec = (M % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const int choice = cov_kernel_choice();
+    p.tc = M > 0 && M % 4 == 0 && choice != 1 && (choice == 2 || M >= 128);
     return p;
 }
 
 int64_t cov_tslice(const CovPlan& p, int64_t rows) {
+    if (p.tc) return cov_i8_run_length(p.M, rows);
     if (rows <= 0) return kTT;
     const int64_t target = std::max<int64_t>(1, (int64_t)(p.vec ? 8 : 4) * num_sms() / p.npairs);
     const int64_t S = std::min<int64_t>(target, ceil_div(rows, kTT));
@@ -653,6 +670,7 @@ int64_t cov_slices(const CovPlan& p, int64_t rows) {
 }
 
 size_t cov_partials_bytes(const CovPlan& p, int64_t slices) {
+    if (p.tc) return cov_i8_partials_bytes(p.M, slices);
     return (size_t)slices * p.npairs * kCT * kCT * sizeof(double);
 }
 
@@ -660,6 +678,12 @@ void cov_partials(const float* X, int64_t M, int64_t r0, int64_t r1, const CovPl
                   int64_t S, cudaStream_t stream) {
     const int64_t rows = r1 - r0;
     if (rows <= 0 || S <= 0) return;
+    if (p.tc) {  // runs of the plan's length: the slicing the streamed forms use too
+        const int64_t R = cov_tslice(p, rows);
+        if (ceil_div(rows, R) != S) throw_invalid("covariance: slice count does not match the plan");
+        cov_partials_sliced(X, M, r0, r1, p, partials, R, stream);
+        return;
+    }
     cov_partials_sliced(X, M, r0, r1, p, partials, ceil_div(ceil_div(rows, S), kTT) * kTT, stream);
 }
 
@@ -668,6 +692,17 @@ void cov_partials_sliced(const float* X, int64_t M, int64_t r0, int64_t r1, cons
     const int64_t rows = r1 - r0;
     if (rows <= 0) return;
     if (tslice <= 0 || tslice % kTT != 0) throw_invalid("covariance slice length must be a multiple of 32");
+    if (p.tc) {
+        if ((reinterpret_cast<uintptr_t>(X + r0 * M) & 15) == 0) {
+            cov_i8_partials(X, M, r0, r1, tslice, partials, stream);
+        } else {  // the tensor map needs 16-byte aligned rows: work on an aligned copy
+            DevBuf copy(sizeof(float) * (size_t)(rows * M), stream);
+            MS3_CUDA(cudaMemcpyAsync(copy.get(), X + r0 * M, sizeof(float) * (size_t)(rows * M),
+                                     cudaMemcpyDeviceToDevice, stream));
+            cov_i8_partials(copy.as<float>(), M, 0, rows, tslice, partials, stream);
+        }
+        return;
+    }
     const int64_t S = ceil_div(rows, tslice);
     if (p.vec)
         cov_partial8<<<dim3(p.npairs, (unsigned)S), 64, 0, stream>>>(X, M, r0, r1, p.nb, tslice, partials);
@@ -678,6 +713,10 @@ void cov_partials_sliced(const float* X, int64_t M, int64_t r0, int64_t r1, cons
 
 void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, int64_t N, double* XXt,
                 cudaStream_t stream) {
+    if (p.tc) {
+        cov_i8_finish(partials, S, M, N, XXt, stream);
+        return;
+    }
     if (S == 0) {
         MS3_CUDA(cudaMemsetAsync(XXt, 0, sizeof(double) * (size_t)(M * M), stream));
         return;

@@ -16,9 +16,14 @@ void covariance_sum_device(const float* X, int64_t M, int64_t N, double* XXt_sum
 // The covariance in pieces, for callers that stream the rows in: partial
 // tiles of rows [r0, r1) go to `S` slices of a partials buffer; cov_finish
 // sums all slices written so far (fixed order) and divides by N-1.
+// tc: the tensor-core kernel (exact int8 digit products, cov_i8.cu), whose
+// slices are runs of cov_tslice timepoints with one partial tile per 128 x
+// 128 channel block pair; otherwise the FP32-FMA kernel (64 x 64 tiles).
 struct CovPlan {
     int nb = 0, npairs = 0;
     bool vec = false;
+    bool tc = false;
+    int64_t M = 0;
 };
 CovPlan cov_plan(const float* X, int64_t M);
 int64_t cov_slices(const CovPlan& p, int64_t rows);
@@ -34,6 +39,20 @@ void cov_partials_sliced(const float* X, int64_t M, int64_t r0, int64_t r1, cons
                          int64_t tslice, cudaStream_t stream);
 void cov_finish(const double* partials, int64_t S, const CovPlan& p, int64_t M, int64_t N, double* XXt,
                 cudaStream_t stream);
+
+// Tensor-core covariance pieces (cov_i8.cu): runs of R timepoints (a
+// multiple of 32, at most 32768) of rows [r0, r1) of X, one FP64 partial tile
+// per (run, block pair); finish sums `runs` runs in order.  X + r0 * M must
+// be 16-byte aligned with M % 4 == 0.
+int cov_i8_pairs(int64_t M);
+int64_t cov_i8_run_length(int64_t M, int64_t rows);
+size_t cov_i8_partials_bytes(int64_t M, int64_t runs);
+void cov_i8_partials(const float* X, int64_t M, int64_t r0, int64_t r1, int64_t R, double* partials,
+                     cudaStream_t stream);
+void cov_i8_finish(const double* partials, int64_t runs, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
+// Raises MS3GPU_ERR_CUDA (after a synchronize) when a tensor-core covariance
+// pipeline wait gave up, and clears the flag.
+void covariance_check_timeout(cudaStream_t stream);
 
 // The same covariance with its partial sums in a fixed 16 MiB device array
 // instead of allocated scratch (X and XXt must be device memory).

@@ -131,15 +131,20 @@ def test_whiten_stream_equals_in_memory(gpu_lib, M, N, q, precision):
 
 
 def test_whiten_stream_slab_below_one_slice(gpu_lib):
-    # blocks of 1024 timepoints, below one covariance slice of the whole
-    # recording (5376 timepoints): only the FP64 summation order differs
+    # blocks of 1024 timepoints, below one covariance run of the whole
+    # recording: the runs shrink to the block, so each channel's fixed-point
+    # scale is taken over 1024 timepoints instead of a whole run.  The
+    # covariance stays within its 1e-8 tolerance; at 384 channels the
+    # whitening matrix amplifies such differences (~30x) and the 1e-4
+    # rounding turns them into whole rounding steps, so the outputs agree to
+    # the plain-form tolerance rather than bit for bit.
     M, N = 384, 300000
     X = api.bandpass_filter(synth.generate_numpy(M, N, K=10, seed=9), FS, FMIN, FMAX, FWID, num_threads=16)
     ref = api.whiten(X)
     rec = Recorder(X, N, M, np.float32)
     api.whiten_stream(rec.source, rec.sink, M, N, slab_bytes=1024 * M * 4)
     assert rec.written.all()
-    assert o64.rel_l2(rec.Y, ref) <= 1e-6
+    assert o64.rel_l2(rec.Y, ref) <= 1e-5
 
 
 def test_stream_callback_failures(gpu_lib):

@@ -6,9 +6,10 @@ processing starts, and streaming loops that must not stall on a device
 allocation.  It keeps its partial sums in a fixed 16 MiB array inside the
 library's device image.  These tests call it through the C ABI with device
 buffers and compare it, on two calls in a row, with the allocating entry
-point (ms3gpu_whiten_covariance; 1e-12 relative, the two differ only in the
-order of FP64 partial sums) and with the oracle's covariance pass on the same
-input (1e-8 relative, the covariance tolerance of the other tests).  The call
+point (ms3gpu_whiten_covariance) and with the oracle's covariance pass on the
+same input, both within 1e-8 relative, the covariance tolerance of the other
+tests (from 128 channels on the allocating entry point sums on the tensor
+cores with its own exact-integer arithmetic, so the two are not bit-equal).  The call
 only queues its work on the stream, so the tests read the result after the
 stream has reached it.  The file sorts last so that a run stopping at its
 first failure has already run every other test.
@@ -45,7 +46,7 @@ def test_noalloc_covariance_matches_allocating_entry_point(gpu_lib, ref32, M, N)
         torch.cuda.current_stream().synchronize()  # the call returns before its work is done
         got = out.cpu().numpy().T  # column-major buffer -> matrix notation
         assert np.all(np.isfinite(got))
-        assert o64.rel_l2(got, ref) <= 1e-12
+        assert o64.rel_l2(got, ref) <= 1e-8
         assert o64.rel_l2(got, oracle) <= 1e-8
         np.testing.assert_array_equal(got, got.T)
 
