@@ -321,6 +321,109 @@ def replica_throughput(world, M, N, steps, ms_total):
 
 # ----------------------------------------------------------------- GPU arm
 
+def _event_ms(fn, stream, reps):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def mixed_record(ms, synth, dev, stream):
+    """Plain and mixed forms of bandpass+whiten on the 32 x 1.8M recording
+    (device-resident, CUDA events), with the mixed form's error against the
+    FP64 oracle."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle64
+
+    M, N = 32, 1_800_000
+    Xh = synth.generate_numpy(M, N, K=20, seed=0, sites=(3, 6))
+    X = torch.from_numpy(Xh).to(dev)
+    out = torch.empty_like(X)
+    t_plain = _event_ms(lambda: ms.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=out), stream, 5)
+    t_mixed = _event_ms(lambda: ms.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=out,
+                                                   precision="mixed"), stream, 5)
+    pre_mixed = out.cpu().numpy()
+    _, q64, _, _ = oracle64.whiten(oracle64.bandpass_filter(Xh, FS, FMIN, FMAX, FWID, num_threads=GEOM_T))
+    return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1 data",
+            "plain_ms": t_plain, "mixed_ms": t_mixed, "plain_gchs": M * N / t_plain / 1e6,
+            "mixed_gchs": M * N / t_mixed / 1e6, "mixed_over_plain": t_plain / t_mixed,
+            "mixed_rel_l2_vs_fp64": oracle64.rel_l2(pre_mixed, q64),
+            "mixed_max_abs_vs_fp64": float(np.max(np.abs(pre_mixed - q64))),
+            "gate_rel_l2": 1e-4}
+
+
+def c4_jobs(seed=1):
+    """The batched uneven workload: 48 recordings, channel counts from
+    {16, 32, 64, 128, 384}, durations uniform 30 s - 20 min, sample rates from
+    {20, 30} kHz, freq_max = min(6000, 0.4 fs)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(48):
+        M = int(rng.choice([16, 32, 64, 128, 384]))
+        fs = float(rng.choice([20000.0, 30000.0]))
+        N = int(round(rng.uniform(30.0, 1200.0) * fs))
+        jobs.append((M, N, fs, min(6000.0, 0.4 * fs)))
+    return jobs
+
+
+def c4_record(ms, synth, dev, stream, budget_bytes=60 << 30):
+    """Times the 48-recording workload in groups whose inputs and outputs fit
+    `budget_bytes` of device memory: per group, one batched call against the
+    same recordings one call at a time (both device-resident, CUDA events).
+    Recordings are generated on the device per group (not timed)."""
+    import torch
+
+    jobs = c4_jobs()
+    groups, cur, used = [], [], 0
+    for j in sorted(jobs, key=lambda j: j[0] * j[1]):
+        b = 8 * j[0] * j[1]
+        if cur and used + b > budget_bytes:
+            groups.append(cur)
+            cur, used = [], 0
+        cur.append(j)
+        used += b
+    if cur:
+        groups.append(cur)
+    t_batch = t_single = 0.0
+    total = 0
+    for gi, grp in enumerate(groups):
+        recs = []
+        for k, (M, N, fs, fmax) in enumerate(grp):
+            X = synth.generate_torch(M, N, fs=fs, K=max(4, M // 2), seed=100 + gi * 64 + k,
+                                     sites=(6, 12) if M >= 64 else (3, 6), device=dev)
+            recs.append({"X": X, "samplerate": fs, "freq_min": FMIN, "freq_max": fmax, "freq_wid": FWID,
+                         "num_threads": GEOM_T})
+            total += M * N
+        t_batch += _event_ms(lambda: ms.bandpass_whiten_batch(recs), stream, 1)
+        outs = [torch.empty_like(r["X"]) for r in recs]
+
+        def singles():
+            for r, o in zip(recs, outs):
+                ms.bandpass_whiten(r["X"], r["samplerate"], r["freq_min"], r["freq_max"], r["freq_wid"],
+                                   num_threads=GEOM_T, out=o)
+
+        t_single += _event_ms(singles, stream, 1)
+        del recs, outs
+        torch.cuda.empty_cache()
+    return {"workload": "48 recordings, M in {16,32,64,128,384}, 30 s - 20 min, 20/30 kHz, seed 1",
+            "ch_samples": total, "groups": len(groups), "batch_ms": t_batch, "single_ms": t_single,
+            "batch_gchs": total / t_batch / 1e6, "single_gchs": total / t_single / 1e6,
+            "batch_over_single": t_single / t_batch}
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,6 +435,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--c4", action="store_true",
+                    help="also time the batched uneven workload (48 recordings, 30 s - 20 min) in memory-bounded "
+                         "groups: several minutes")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -442,6 +549,20 @@ def main():
                     "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
                     "algorithmic_bytes_per_ch_sample": algo_bytes[dom], "stage_ms": stages}
 
+    # ---- the whole step against the fused path's compulsory traffic (12 B per ch-sample)
+    step_roofline = {"bytes_per_ch_sample": 12, "achieved": 12 * M * N / (ms_step / 1e3) / 1e9, "peak": hbm_peak,
+                     "unit": "GB/s", "peak_source": peak_src}
+    step_roofline["frac"] = step_roofline["achieved"] / hbm_peak
+
+    # ---- mixed-precision form on the config-1 data, next to the plain form (FP64 oracle for its error)
+    mixed = None
+    if rank == 0 and not args.no_mixed:
+        mixed = mixed_record(ms, synth, dev, stream)
+
+    c4 = None
+    if args.c4 and rank == 0:
+        c4 = c4_record(ms, synth, dev, stream)
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -481,6 +602,9 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "roofline": roofline,
+            "step_roofline": step_roofline,
+            "mixed": mixed,
+            "batched_c4": c4,
             "cpu_baseline": cpu,
             "e2e": e2e,
         }

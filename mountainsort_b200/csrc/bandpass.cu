@@ -41,6 +41,7 @@
 #include "common.cuh"
 #include "fft_block.cuh"
 #include "fft_reg.cuh"
+#include "host_dft.h"
 #include "ms3gpu.h"
 #include "tc_sm100.cuh"
 
@@ -61,7 +62,8 @@ struct Geom {
     int ngroups;
     int64_t c_begin;     // first window of this call
     int64_t nwin;        // windows in this call
-    int64_t L, L1, L2;
+    int64_t L, L1, L2;   // FFT length and its factors
+    int64_t Lw;          // window length chunk + 120000 (< L when the window is zero-padded to a longer FFT)
     int64_t chunk;
     int sub;
     int64_t N2;          // output timepoints
@@ -71,6 +73,15 @@ struct Geom {
 };
 
 // ---------------------------------------------------------------- kernels
+
+// v * kernel[k] / L for the kernel value held as hi + lo floats: the product
+// rounds once to float like the reference's float *= double
+// (p_bandpass_filter.cpp:87-95) instead of after a rounding of the kernel
+// value itself, which would be the same relative error in every window and
+// channel at that frequency.
+__device__ __forceinline__ float2 kern_mul(float2 v, float2 k) {
+    return make_float2(__fmaf_rn(v.x, k.x, __fmul_rn(v.x, k.y)), __fmaf_rn(v.y, k.x, __fmul_rn(v.y, k.y)));
+}
 
 __device__ __forceinline__ float2 load_signal(const void* __restrict__ raw, const Geom& g, int64_t t, int64_t s) {
     if (t < 0 || t >= g.N || s >= g.P) return make_float2(0.f, 0.f);
@@ -135,7 +146,9 @@ __global__ void __launch_bounds__(kThreads) bp_cols_forward(const void* __restri
     for (int idx = threadIdx.x; idx < n1len * G; idx += blockDim.x) {
         const int n1 = idx >> g.log2G;
         const int gi = idx & (G - 1);
-        bufA[idx] = load_signal(raw, g, t0 + (int64_t)n1 * g.L2, (int64_t)grp * G + gi);
+        const int64_t n = (int64_t)n1 * g.L2 + n2;  // window index
+        bufA[idx] = n < g.Lw ? load_signal(raw, g, t0 + (int64_t)n1 * g.L2, (int64_t)grp * G + gi)
+                             : make_float2(0.f, 0.f);
     }
     __syncthreads();
     float2* res = fft_smem<false>(bufA, bufB, twS, plan, g.log2G);
@@ -152,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) bp_cols_forward(const void* __restri
 __global__ void __launch_bounds__(kThreads) bp_rows_filter(float2* __restrict__ scratch, Geom g, SubFft P2,
                                                            const float2* __restrict__ tw2,
                                                            const float2* __restrict__ twL,
-                                                           const float* __restrict__ kern) {
+                                                           const float2* __restrict__ kern) {
     extern __shared__ float4 smem_f4[];
     float2* smem = reinterpret_cast<float2*>(smem_f4);
     __shared__ SubFft plan;
@@ -167,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) bp_rows_filter(float2* __restrict__ 
     const int k1 = blockIdx.x;
     float2* row = scratch + (size_t)blockIdx.y * (size_t)(g.L * G) + (((size_t)k1 * g.L2) << g.log2G);
     const float2* twrow = twL + (size_t)k1 * g.L2;
-    const float* krow = kern + (size_t)k1 * g.L2;
+    const float2* krow = kern + (size_t)k1 * g.L2;
     for (int idx = threadIdx.x; idx < n2len * G; idx += blockDim.x) {
         const int n2 = idx >> g.log2G;
         bufA[idx] = cmul(row[idx], twrow[n2]);
@@ -176,9 +189,7 @@ __global__ void __launch_bounds__(kThreads) bp_rows_filter(float2* __restrict__ 
     float2* res = fft_smem<false>(bufA, bufB, twS, plan, g.log2G);
     float2* other = (res == bufA) ? bufB : bufA;
     for (int idx = threadIdx.x; idx < n2len * G; idx += blockDim.x) {
-        const float kv = krow[idx >> g.log2G];
-        float2 v = res[idx];
-        res[idx] = make_float2(v.x * kv, v.y * kv);
+        res[idx] = kern_mul(res[idx], krow[idx >> g.log2G]);
     }
     __syncthreads();
     float2* res2 = fft_smem<true>(res, other, twS, plan, g.log2G);
@@ -369,7 +380,7 @@ template <int SA, int SB>
 __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scratch, Geom g,
                                                        const float2* __restrict__ roots,
                                                        const float2* __restrict__ twL,
-                                                       const float* __restrict__ kern) {
+                                                       const float2* __restrict__ kern) {
     constexpr int n = SA * SB;
     extern __shared__ float4 smem_f4[];
     float2* buf = reinterpret_cast<float2*>(smem_f4);
@@ -379,7 +390,7 @@ __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scra
     const int k1 = blockIdx.x;
     float2* row = scratch + (size_t)blockIdx.y * (size_t)(g.L * G) + (((size_t)k1 * g.L2) << g.log2G);
     const float2* twrow = twL + (size_t)k1 * g.L2;
-    const float* krow = kern + (size_t)k1 * g.L2;
+    const float2* krow = kern + (size_t)k1 * g.L2;
     // forward pass 1 (radix SA over items i < SB)
     for (int it = threadIdx.x; it < (SB << g.log2G); it += blockDim.x) {
         const int gi = it & (G - 1), i = it >> g.log2G;
@@ -407,10 +418,7 @@ __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scra
         }
         RegDft<SB, false>::run(u);
 #pragma unroll
-        for (int q = 0; q < SB; q++) {
-            const float kv = __ldg(&krow[i + q * SA]);
-            u[q] = make_float2(u[q].x * kv, u[q].y * kv);
-        }
+        for (int q = 0; q < SB; q++) u[q] = kern_mul(u[q], __ldg(&krow[i + q * SA]));
         RegDft<SB, true>::run(u);
     }
     __syncthreads();
@@ -463,7 +471,7 @@ struct F2Pipe {
     static constexpr int G = 16;
     static constexpr int kRowBytes = n * G * 8;
     static constexpr int kTwBytes = n * 8;
-    static constexpr int kKernBytes = n * 4;
+    static constexpr int kKernBytes = n * 8;  // (hi, lo) per bin
     static constexpr int kSlotBytes = kRowBytes + kTwBytes + kKernBytes;
     static constexpr size_t kSmemBytes = (size_t)kF2Ring * kSlotBytes + n * 8 + kF2Ring * 8;
     static_assert(kRowBytes % 16 == 0 && kTwBytes % 16 == 0 && kKernBytes % 16 == 0, "bulk copies need 16-byte sizes");
@@ -473,7 +481,7 @@ struct F2Pipe {
 template <int SA, int SB>
 __global__ void __launch_bounds__(kF2Threads, 1)
     bpr_rows_filter_pipe(float2* __restrict__ scratch, Geom g, const float2* __restrict__ roots,
-                         const float2* __restrict__ twL, const float* __restrict__ kern, int64_t nrows) {
+                         const float2* __restrict__ twL, const float2* __restrict__ kern, int64_t nrows) {
     using P = F2Pipe<SA, SB>;
     constexpr int n = P::n, G = P::G;
     extern __shared__ float4 smem_f4[];
@@ -519,7 +527,7 @@ __global__ void __launch_bounds__(kF2Threads, 1)
         uint8_t* slot = slot_ptr(j);
         float2* buf = reinterpret_cast<float2*>(slot);
         const float2* tw = reinterpret_cast<const float2*>(slot + P::kRowBytes);
-        const float* kr = reinterpret_cast<const float*>(slot + P::kRowBytes + P::kTwBytes);
+        const float2* kr = reinterpret_cast<const float2*>(slot + P::kRowBytes + P::kTwBytes);
         // forward pass 1 (radix SA over items i < SB), in place
         float2 u[SA];
         if (outer) {
@@ -546,10 +554,7 @@ __global__ void __launch_bounds__(kF2Threads, 1)
             }
             RegDft<SB, false>::run(v);
 #pragma unroll
-            for (int q = 0; q < SB; q++) {
-                const float kv = kr[i + q * SA];
-                v[q] = make_float2(v[q].x * kv, v[q].y * kv);
-            }
+            for (int q = 0; q < SB; q++) v[q] = kern_mul(v[q], kr[i + q * SA]);
             RegDft<SB, true>::run(v);
         }
         __syncthreads();
@@ -716,13 +721,14 @@ size_t smem_bytes_for(int n, int G, int twlen) {
 // Device-resident tables for one (L, filter) combination.
 struct BandpassPlan {
     int device = -1;
-    int64_t L = 0, L1 = 0, L2 = 0;
+    int64_t L = 0, L1 = 0, L2 = 0;  // FFT length = L1 * L2
+    int64_t Lw = 0;                 // window length (L == Lw unless the window is zero-padded)
     int paired = 1;
     SubFft P1{}, P2{};
     float2* tw1 = nullptr;  // P1 twiddles
     float2* tw2 = nullptr;  // P2 twiddles
     float2* twL = nullptr;  // [k1][n2] exp(-2 pi i n2 k1 / L)
-    float* kern = nullptr;  // [k1][k2] kernel[k1 + L1 k2] / L
+    float2* kern = nullptr;  // [k1][k2] kernel[k1 + L1 k2] / L as (hi, lo) floats
     float2* root1 = nullptr;  // exp(-2 pi i e / L1), e < L1
     float2* root2 = nullptr;  // exp(-2 pi i e / L2), e < L2
     bool fast = false;        // L1 x L2 = 480 x 500: register-pass kernels
@@ -756,61 +762,100 @@ bool factor_window(int64_t L, int64_t& L1, int64_t& L2) {
     return true;
 }
 
-std::shared_ptr<BandpassPlan> build_plan(int64_t L, double fs, double fmin, double fmax, double fwid) {
+// The band kernel of a window of length n (define_kernel,
+// p_bandpass_filter.cpp:421-447), in FP64.
+std::vector<double> band_kernel(int64_t n, double fs, double fmin, double fmax, double fwid) {
+    std::vector<double> K((size_t)n);
+    const double T = n / fs;
+    const double df = 1 / T;
+    for (int64_t i = 0; i < n; i++) {
+        const double fgrid = (i <= (n + 1) / 2) ? df * i : df * (i - n);
+        const double absf = std::fabs(fgrid);
+        double val = 1.0;
+        if (fmin != 0) {
+            if (i == 0)
+                val = 0.0;
+            else
+                val *= (1 + std::erf(3.0 * (absf - fmin) / fmin)) / 2;
+        }
+        if (fmax != 0) val *= (1 - std::erf((absf - fmax) / fwid)) / 2;
+        K[(size_t)i] = std::sqrt(val);
+    }
+    return K;
+}
+
+// Lw: the reference's window length (chunk + 120000).  When Lw factors into
+// primes up to 64 the FFT has length Lw and the kernel is kernel / Lw, as in
+// the reference.  Otherwise (a prime factor above 64, e.g. Lw = 466033 or
+// 1398101 = 23 * 89 * 683) the window's circular convolution is done with an
+// FFT of a 5-smooth length L >= 2 Lw - 1: the reference computes, per window,
+//     y = Re(IDFT(kernel .* DFT(x))) / Lw = x (*) h  (circular, length Lw),
+//     h[j] = Re(sum_k kernel[k] exp(2 pi i j k / Lw)) / Lw   (real, even),
+// and with the window zero-padded to L and the taps laid out as g[j] = h[j],
+// g[L - j] = h[j] (0 < j < Lw), the length-L circular convolution x (*) g
+// equals y on [0, Lw) because L >= 2 Lw - 1 leaves no wrap-around.  g is
+// symmetric, so DFT_L(g) is real and even and the L-point plan applies it as
+// it applies the band kernel (channel pairs included).  h and DFT_L(g) are
+// formed in FP64 on the host.
+std::shared_ptr<BandpassPlan> build_plan(int64_t Lw, double fs, double fmin, double fmax, double fwid) {
+    constexpr int64_t kMaxRow = 8192;  // longest row transform of a zero-padded plan (shared memory)
     auto plan = std::make_shared<BandpassPlan>();
     MS3_CUDA(cudaGetDevice(&plan->device));
+    plan->Lw = Lw;
+    const std::vector<double> Kw = band_kernel(Lw, fs, fmin, fmax, fwid);
+    std::vector<double> KF;  // the kernel applied to the L-point spectrum, including the 1/L
+    int64_t L = Lw;
+    if (factor_window(Lw, plan->L1, plan->L2) && plan->L2 <= 16384) {
+        KF.resize((size_t)Lw);
+        for (int64_t i = 0; i < Lw; i++) KF[(size_t)i] = Kw[(size_t)i] * (1.0 / Lw);
+    } else {
+        L = hostdft::next_smooth5(2 * Lw - 1);
+        while (!(factor_window(L, plan->L1, plan->L2) && plan->L2 <= kMaxRow)) L = hostdft::next_smooth5(L + 1);
+        std::vector<hostdft::cd> kc((size_t)Lw);
+        for (int64_t i = 0; i < Lw; i++) kc[(size_t)i] = Kw[(size_t)i];
+        const std::vector<hostdft::cd> hc = hostdft::dft(kc, +1);
+        std::vector<hostdft::cd> g((size_t)L, hostdft::cd(0));
+        for (int64_t j = 0; j < Lw; j++) {
+            const double h = hc[(size_t)j].real() / (double)Lw;
+            g[(size_t)j] = h;
+            if (j > 0) g[(size_t)(L - j)] = h;
+        }
+        const std::vector<hostdft::cd> G = hostdft::dft(g, -1);
+        KF.resize((size_t)L);
+        for (int64_t i = 0; i < L; i++) KF[(size_t)i] = G[(size_t)i].real() / (double)L;
+        for (int64_t i = 1; i < L; i++) KF[(size_t)i] = KF[(size_t)(L - i)] = 0.5 * (KF[(size_t)i] + KF[(size_t)(L - i)]);
+    }
     plan->L = L;
-    if (!factor_window(L, plan->L1, plan->L2))
-        throw_unsupported("FFT window length " + std::to_string(L) +
-                          " has a prime factor above 64; not supported by the GPU path");
-    if (plan->L2 > 16384)
-        throw_unsupported("FFT window length " + std::to_string(L) + " needs a factor above 16384");
     const int64_t L1 = plan->L1, L2 = plan->L2;
     std::vector<float2> tw1, tw2;
     plan->P1 = make_subfft((int)L1, tw1);
     plan->P2 = make_subfft((int)L2, tw2);
 
-    // band kernel (define_kernel, p_bandpass_filter.cpp:421-447)
-    std::vector<double> K((size_t)L);
-    {
-        const double T = L / fs;
-        const double df = 1 / T;
-        for (int64_t i = 0; i < L; i++) {
-            const double fgrid = (i <= (L + 1) / 2) ? df * i : df * (i - L);
-            const double absf = std::fabs(fgrid);
-            double val = 1.0;
-            if (fmin != 0) {
-                if (i == 0)
-                    val = 0.0;
-                else
-                    val *= (1 + std::erf(3.0 * (absf - fmin) / fmin)) / 2;
-            }
-            if (fmax != 0) val *= (1 - std::erf((absf - fmax) / fwid)) / 2;
-            K[(size_t)i] = std::sqrt(val);
-        }
-    }
     // Two channels can share one complex transform only if the kernel is even.
     plan->paired = 1;
     for (int64_t i = 1; i < L; i++)
-        if (K[(size_t)i] != K[(size_t)(L - i)]) { plan->paired = 0; break; }
+        if (KF[(size_t)i] != KF[(size_t)(L - i)]) { plan->paired = 0; break; }
+    if (const char* up = std::getenv("MS3GPU_BP_UNPAIRED"))  // one channel per complex signal (testing)
+        if (up[0] == '1') plan->paired = 0;
 
-    const double factor = 1.0 / L;
-    std::vector<float> kern((size_t)L);
+    std::vector<float2> kern((size_t)L);
     std::vector<float2> twL((size_t)L);
     for (int64_t k1 = 0; k1 < L1; k1++)
         for (int64_t j = 0; j < L2; j++) {
-            kern[(size_t)(k1 * L2 + j)] = (float)(K[(size_t)(k1 + L1 * j)] * factor);
+            const double kd = KF[(size_t)(k1 + L1 * j)];
+            const float hi = (float)kd;
+            kern[(size_t)(k1 * L2 + j)] = make_float2(hi, (float)(kd - (double)hi));
             const double a = -2.0 * M_PI * (double)(j * k1) / (double)L;
             twL[(size_t)(k1 * L2 + j)] = make_float2((float)std::cos(a), (float)std::sin(a));
         }
     MS3_CUDA(cudaMalloc(&plan->tw1, std::max<size_t>(1, tw1.size()) * sizeof(float2)));
     MS3_CUDA(cudaMalloc(&plan->tw2, std::max<size_t>(1, tw2.size()) * sizeof(float2)));
     MS3_CUDA(cudaMalloc(&plan->twL, (size_t)L * sizeof(float2)));
-    MS3_CUDA(cudaMalloc(&plan->kern, (size_t)L * sizeof(float)));
+    MS3_CUDA(cudaMalloc(&plan->kern, (size_t)L * sizeof(float2)));
     if (!tw1.empty()) MS3_CUDA(cudaMemcpy(plan->tw1, tw1.data(), tw1.size() * sizeof(float2), cudaMemcpyHostToDevice));
     if (!tw2.empty()) MS3_CUDA(cudaMemcpy(plan->tw2, tw2.data(), tw2.size() * sizeof(float2), cudaMemcpyHostToDevice));
     MS3_CUDA(cudaMemcpy(plan->twL, twL.data(), (size_t)L * sizeof(float2), cudaMemcpyHostToDevice));
-    MS3_CUDA(cudaMemcpy(plan->kern, kern.data(), (size_t)L * sizeof(float), cudaMemcpyHostToDevice));
+    MS3_CUDA(cudaMemcpy(plan->kern, kern.data(), (size_t)L * sizeof(float2), cudaMemcpyHostToDevice));
     auto roots = [](int64_t n) {
         std::vector<float2> r((size_t)n);
         for (int64_t e = 0; e < n; e++) {
@@ -892,8 +937,9 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
     if (M <= 0 || N2 <= 0) return;
     if (bp.num_threads < 1) throw_invalid("num_threads must be >= 1");
     const int64_t chunk = bandpass_chunk_size(M, bp.num_threads);
-    const int64_t L = chunk + 2 * kOverlap;
-    auto plan = get_plan(L, bp.samplerate, bp.freq_min, bp.freq_max, bp.freq_wid);
+    const int64_t Lw = chunk + 2 * kOverlap;
+    auto plan = get_plan(Lw, bp.samplerate, bp.freq_min, bp.freq_max, bp.freq_wid);
+    const int64_t L = plan->L;  // FFT length (Lw, or a zero-padded length)
 
     Geom g{};
     g.M = M;
@@ -906,6 +952,7 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
     g.m_even = (M % 2 == 0) && ((uintptr_t)raw % (in_i16 ? 4 : 8) == 0) &&
                (out_i16 || ((uintptr_t)out % 8 == 0));
     g.L = L;
+    g.Lw = Lw;
     g.L1 = plan->L1;
     g.L2 = plan->L2;
     g.chunk = chunk;

@@ -31,9 +31,9 @@
 //               bj) into a 3-stage ring
 //   warp 1      TMEM allocation (512 columns: four 128 x 128 int32
 //               accumulators); one thread issues the ten MMAs per stage
-//   warps 2-13  convert fp32 tiles to the four digit planes in the UMMA
+//   warps 2-17  convert fp32 tiles to the four digit planes in the UMMA
 //               MN-major 128-byte-swizzle layout (3-stage ring)
-//   warps 14-17 at the end of each run: read the accumulators, combine,
+//   warps 18-21 at the end of each run: read the accumulators, combine,
 //               scale, store the run's FP64 partial tile
 // Every mbarrier wait is bounded (tc::mbar_wait); a timeout sets
 // g_cov_timeout, which the host checks after the call.
@@ -66,8 +66,9 @@ constexpr int kF32Bytes = kKT * kB * 4;       // 16 KB: one block's fp32 tile
 constexpr int kPlaneBytes = kKT * kB;         // 4 KB: one digit plane of one block
 constexpr int kF32Stage = 2 * kF32Bytes;      // blocks bi and bj
 constexpr int kPlaneStage = 2 * 4 * kPlaneBytes;
-constexpr int kConvWarps = 12;
-constexpr int kThreads = (2 + kConvWarps + 4) * 32;  // 576
+constexpr int kConvWarps = 16;
+constexpr int kThreads = (2 + kConvWarps + 4) * 32;  // 704
+static_assert(kKT == 2 * kConvWarps, "each converter thread takes two rows of a stage");
 constexpr int kSentinel = 1000;               // scale exponent of a channel whose run holds inf / NaN
 constexpr size_t kSmemBytes = (size_t)kS1 * kF32Stage + (size_t)kS2 * kPlaneStage + 2 * kB * sizeof(int) +
                               1024 /*align*/ + 256 /*barriers*/;
@@ -161,6 +162,14 @@ __device__ __forceinline__ uint32_t gather_byte(const uint32_t (&v)[4]) {
     return __byte_perm(a, b, 0x5410);
 }
 
+// 32 lanes x 8 consecutive 32-bit TMEM columns (thread i: row lane base + i).
+__device__ __forceinline__ void tmem_ld_32x32b_x8(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ int sext8(uint32_t b) { return (int)(int8_t)(uint8_t)(b & 0xFFu); }
 
 // Shared-memory descriptor of one digit plane: MN-major, 128-byte swizzle,
@@ -189,6 +198,49 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %4, p;\n\t}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(kIdescI8)
         : "memory");
+}
+
+// One stage of the converter warps: thread (tg, q) turns rows tg and tg + 16
+// of each block's fp32 tile (channels 4q .. 4q + 3) into the four digit
+// planes; all its loads are issued before the arithmetic.  DIAG: one block
+// (bi == bj), whose d2^2 sums go to dsum.
+template <int NBLK, bool DIAG>
+__device__ __forceinline__ void convert_stage(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int tg,
+                                              int q, const float (&m8)[2][4], const float (&mult)[2][4],
+                                              int (&dsum)[4]) {
+    float4 x[NBLK][2];
+#pragma unroll
+    for (int b = 0; b < NBLK; b++)
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            x[b][h] = *reinterpret_cast<const float4*>(src + (size_t)b * kF32Bytes + (tg + 16 * h) * (kB * 4) + q * 16);
+#pragma unroll
+    for (int b = 0; b < NBLK; b++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int t = tg + 16 * h;
+            uint32_t w[4], lo[4];
+            digits4(x[b][h], m8[b], mult[b], w, lo);
+            const uint32_t p0 = gather_byte<2>(w);
+            const uint32_t p1 = gather_byte<1>(w) ^ 0x80808080u;
+            const uint32_t p2 = gather_byte<0>(w) ^ 0x80808080u;
+            const uint32_t p3 = gather_byte<0>(lo);
+            if (DIAG) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int d2 = sext8(p2 >> (8 * c));
+                    dsum[c] += d2 * d2;
+                }
+            }
+            const int r8 = t & 7;
+            const size_t off = (size_t)(t >> 3) * 1024 + r8 * 128 + (((q >> 2) ^ r8) << 4) + ((q & 3) << 2);
+            uint8_t* pl = dst + (size_t)b * 4 * kPlaneBytes + off;
+            *reinterpret_cast<uint32_t*>(pl) = p0;
+            *reinterpret_cast<uint32_t*>(pl + kPlaneBytes) = p1;
+            *reinterpret_cast<uint32_t*>(pl + 2 * kPlaneBytes) = p2;
+            *reinterpret_cast<uint32_t*>(pl + 3 * kPlaneBytes) = p3;
+        }
+    }
 }
 
 struct Item {
@@ -323,13 +375,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp < 2 + kConvWarps) {
         const int tid = threadIdx.x - 64;
         const int q = tid & 31;   // channel quad within a block: channels 4q .. 4q+3
-        const int tg = tid >> 5;  // rows tg, tg + kConvWarps, ... of each stage
+        const int tg = tid >> 5;  // rows tg and tg + 16 of each stage
         int64_t g = 0;
         bool ok = true;
         for (int64_t i = 0; i < my_items && ok; i++) {
             const Item it = item_of(i);
             const bool diag = it.bi == it.bj;
-            const int nblk = diag ? 1 : 2;
             float mult[2][4], m8[2][4];
 #pragma unroll
             for (int b = 0; b < 2; b++) {
@@ -353,34 +404,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 const uint8_t* src = f32 + (size_t)s1 * kF32Stage;
                 uint8_t* dst = planes + (size_t)s2 * kPlaneStage;
-                for (int b = 0; b < nblk; b++) {
-#pragma unroll
-                    for (int t = tg; t < kKT; t += kConvWarps) {
-                        const float4 x =
-                            *reinterpret_cast<const float4*>(src + (size_t)b * kF32Bytes + t * (kB * 4) + q * 16);
-                        uint32_t w[4], lo[4];
-                        digits4(x, m8[b], mult[b], w, lo);
-                        const uint32_t p0 = gather_byte<2>(w);
-                        const uint32_t p1 = gather_byte<1>(w) ^ 0x80808080u;
-                        const uint32_t p2 = gather_byte<0>(w) ^ 0x80808080u;
-                        const uint32_t p3 = gather_byte<0>(lo);
-                        if (diag) {
-#pragma unroll
-                            for (int c = 0; c < 4; c++) {
-                                const int d2 = sext8(p2 >> (8 * c));
-                                dsum[c] += d2 * d2;
-                            }
-                        }
-                        const int r8 = t & 7;
-                        const size_t off =
-                            (size_t)(t >> 3) * 1024 + r8 * 128 + (((q >> 2) ^ r8) << 4) + ((q & 3) << 2);
-                        uint8_t* pl = dst + (size_t)b * 4 * kPlaneBytes + off;
-                        *reinterpret_cast<uint32_t*>(pl) = p0;
-                        *reinterpret_cast<uint32_t*>(pl + kPlaneBytes) = p1;
-                        *reinterpret_cast<uint32_t*>(pl + 2 * kPlaneBytes) = p2;
-                        *reinterpret_cast<uint32_t*>(pl + 3 * kPlaneBytes) = p3;
-                    }
-                }
+                if (diag)
+                    convert_stage<1, true>(src, dst, tg, q, m8, mult, dsum);
+                else
+                    convert_stage<2, false>(src, dst, tg, q, m8, mult, dsum);
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
@@ -401,7 +428,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (lane == 0) tc::mbar_arrive(&corr_ready[par]);
         }
     } else {
-        // warps 14-17: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows of the tile)
+        // warps 18-21: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows of the tile)
         const int quad = warp & 3;
         const int row = quad * 32 + lane;
         const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
@@ -419,14 +446,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             const unsigned int* mbj = mb + it.r * Mp + (int64_t)it.bj * kB;
             double* dst = partials + ((size_t)it.r * P + it.p) * (kB * kB) + (size_t)row * kB;
 #pragma unroll 1
-            for (int j0 = 0; j0 < kB; j0 += 16) {
-                uint32_t a0[16], a1[16], a2[16], a3[16];
-                tc::tmem_ld_32x32b_x16(taddr + 0 * kB + lane_base + j0, a0);
-                tc::tmem_ld_32x32b_x16(taddr + 1 * kB + lane_base + j0, a1);
-                tc::tmem_ld_32x32b_x16(taddr + 2 * kB + lane_base + j0, a2);
-                tc::tmem_ld_32x32b_x16(taddr + 3 * kB + lane_base + j0, a3);
+            for (int j0 = 0; j0 < kB; j0 += 8) {
+                uint32_t a0[8], a1[8], a2[8], a3[8];
+                tmem_ld_32x32b_x8(taddr + 0 * kB + lane_base + j0, a0);
+                tmem_ld_32x32b_x8(taddr + 1 * kB + lane_base + j0, a1);
+                tmem_ld_32x32b_x8(taddr + 2 * kB + lane_base + j0, a2);
+                tmem_ld_32x32b_x8(taddr + 3 * kB + lane_base + j0, a3);
 #pragma unroll
-                for (int jj = 0; jj < 16; jj += 2) {
+                for (int jj = 0; jj < 8; jj += 2) {
                     double v[2];
 #pragma unroll
                     for (int h = 0; h < 2; h++) {

@@ -267,6 +267,21 @@ __device__ double block_sum(double v, double* red) {
     return t;
 }
 
+// Sum over n < M of f(n), formed by one warp: lane l adds f(l), f(l + 32),
+// ... in order, then a 32-lane XOR tree.  Addition is commutative, so every
+// lane ends with the same bits; both power-iteration kernels form their norms
+// and dot products this way, which keeps their results identical.  The
+// dependent chain is M/32 adds plus five shuffles (the previous per-chunk
+// trees cost five shuffles per 32 elements).
+template <class F>
+__device__ __forceinline__ double warp_ordered_sum(int M, F f) {
+    const int l = threadIdx.x & 31;
+    double t = 0.0;
+    for (int n = l; n < M; n += 32) t += f(n);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return t;
+}
+
 // y = X v for this CTA's rows, written into `dst` of every CTA in the cluster,
 // followed by a cluster barrier.
 __device__ void cluster_matvec(cg::cluster_group& cluster, const double* __restrict__ X, int RS, int r0,
@@ -331,9 +346,8 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
         for (int it = 0; it < num_iter; it++) {
             const int nxt = cur ^ 1;
             cluster_matvec(cluster, X, RS, r0, nr, M, vb[cur], vb[nxt]);
-            double part = 0.0;
-            for (int n = threadIdx.x; n < M; n += blockDim.x) part += vb[nxt][n] * vb[nxt][n];
-            sig = sqrt(block_sum(part, red));
+            const double* y = vb[nxt];
+            sig = sqrt(warp_ordered_sum(M, [&](int n) { return y[n] * y[n]; }));
             __syncthreads();
             if (sig != 0.0)
                 for (int n = threadIdx.x; n < M; n += blockDim.x) vb[nxt][n] = vb[nxt][n] / sig;
@@ -348,9 +362,7 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
         // deflation: X <- X - v u' - u v' + (v'u) v v',  u = X v
         double* u = vb[cur ^ 1];
         cluster_matvec(cluster, X, RS, r0, nr, M, v, u);
-        double part = 0.0;
-        for (int n = threadIdx.x; n < M; n += blockDim.x) part += v[n] * u[n];
-        const double alpha = block_sum(part, red);
+        const double alpha = warp_ordered_sum(M, [&](int n) { return v[n] * u[n]; });
         for (int idx = threadIdx.x; idx < nr * M; idx += blockDim.x) {
             const int r = idx / M, n = idx % M;
             const int m = r0 + r;
@@ -374,21 +386,6 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
 // writes buffer b of its peers only after every CTA has passed the barrier
 // that ended their reads of b.
 constexpr int kPcaWarps = kPcaThreads / 32;
-
-// Sum over n < M of f(n) in the order block_sum forms it when thread n
-// holds f(n): a 32-lane XOR tree per warp, then the warp totals in order.
-template <class F>
-__device__ __forceinline__ double warp_ordered_sum(int M, F f) {
-    const int l = threadIdx.x & 31;
-    double t = 0.0;
-    for (int c = 0; c * 32 < M; c++) {
-        const int n = c * 32 + l;
-        double v = n < M ? f(n) : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        t += v;
-    }
-    return t;
-}
 
 template <int RPW, int CPL>
 __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* __restrict__ XXt, int M,

@@ -252,14 +252,23 @@ def test_fused_pipeline_config1_geometry(gpu_lib, ref32, rec32):
     assert rel(pre, q64) <= 1e-4
 
 
-def test_unsupported_window_is_a_clean_error(gpu_lib):
-    # M=6, T=16 -> L = 466033 (prime): not handled by the GPU factorisation
-    X = np.zeros((1000, 6), np.float32)
-    with pytest.raises(_lib.Ms3GpuError) as e:
-        api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=16)
-    assert e.value.code == _lib.ERR_UNSUPPORTED
-    # the context stays usable
-    api.bandpass_filter(np.zeros((1000, 6), np.float32), FS, FMIN, FMAX, FWID, num_threads=32)
+@pytest.mark.parametrize("M,N,T", [
+    (6, 700000, 16),    # L = 466033, a prime: zero-padded to a 5-smooth FFT of >= 2L - 1 points
+    (4, 1500000, 8),    # L = 1398101 = 23 * 89 * 683 (tetrodes at 8 threads)
+    (5, 300000, 16),    # L = 559240 = 2^3 * 5 * 11 * 31 * 41: factors <= 64, direct
+    (3, 400000, 27),    # odd M (the last pair padded), L = 552336 = 2^4 * 3 * 37 * 311: zero-padded
+])
+def test_bandpass_any_window_length(gpu_lib, ref32, M, N, T):
+    X = synth.generate_numpy(M, N, K=2, seed=M * 13 + T)
+    ref = ref32.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=T)
+    got = api.bandpass_filter(X, FS, FMIN, FMAX, FWID, num_threads=T)
+    e = rel(got, ref)
+    print(f"M={M} T={T} L={ref32.chunk_size(M, T) + 120000}: rel L2 vs ref32 {e:.3e}")
+    assert got.shape == ref.shape
+    assert e <= 1e-5  # gate: plain FP32 form
+    pre = api.whiten(got)
+    pre_ref, _, _ = ref32.whiten(ref)
+    assert rel(pre, pre_ref) <= 1e-5
 
 
 def test_out_of_memory_hook_reports_nomem(gpu_lib):
