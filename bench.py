@@ -362,6 +362,40 @@ def mixed_record(ms, synth, dev, stream):
             "gate_rel_l2": 1e-4}
 
 
+def c5_record(ms, synth, dev, stream):
+    """4 shanks x 384 channels, 5 min at 30 kHz, int16 input (gain 0.195):
+    bandpass on the int16 recording, then each shank whitened on its own
+    (device-resident, CUDA events), plain and mixed forms.  Algorithmic
+    bytes: 2 (int16 read) + 2 (int16 read again for the output pass, were the
+    two fused) + 4 (float write) = 8 per ch-sample."""
+    import numpy as np
+    import torch
+
+    M1, N, S = 384, 9_000_000, 4
+    X16 = torch.empty((N, M1 * S), dtype=torch.int16, device=dev)
+    for k in range(S):
+        Xk = synth.generate_torch(M1, N, K=300, seed=500 + k, sites=(6, 12), device=dev)
+        X16[:, k * M1:(k + 1) * M1] = torch.clamp(torch.round(Xk / 0.195), -32768, 32767).to(torch.int16)
+        del Xk
+    torch.cuda.empty_cache()
+    shanks = [list(range(1 + M1 * k, 1 + M1 * (k + 1))) for k in range(S)]
+    filt = torch.empty((N, M1 * S), dtype=torch.float32, device=dev)
+    pre = torch.empty_like(filt)
+    rec = {"workload": "4 shanks x 384ch x 9M timepoints (5 min @ 30 kHz), int16 input, per-shank whitening"}
+    for prec in ("plain", "mixed"):
+        def run():
+            ms.bandpass_filter(X16, FS, FMIN, FMAX, FWID, num_threads=GEOM_T, out=filt)
+            ms.whiten_blocks(filt, shanks, out=pre, precision=prec)
+        t = _event_ms(run, stream, 2)
+        rec[prec + "_ms"] = t
+        rec[prec + "_gchs"] = M1 * S * N / t / 1e6
+    rec["mixed_over_plain"] = rec["plain_ms"] / rec["mixed_ms"]
+    rec["plain_gbs_at_8B_per_ch_sample"] = 8 * M1 * S * N / (rec["plain_ms"] / 1e3) / 1e9
+    del X16, filt, pre
+    torch.cuda.empty_cache()
+    return rec
+
+
 def c4_jobs(seed=1):
     """The batched uneven workload: 48 recordings, channel counts from
     {16, 32, 64, 128, 384}, durations uniform 30 s - 20 min, sample rates from
@@ -436,6 +470,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--c5", action="store_true",
+                    help="also time the 4 x 384-channel int16 shank configuration (5 min, per-shank whitening)")
     ap.add_argument("--c4", action="store_true",
                     help="also time the batched uneven workload (48 recordings, 30 s - 20 min) in memory-bounded "
                          "groups: several minutes")
@@ -559,10 +595,6 @@ def main():
     if rank == 0 and not args.no_mixed:
         mixed = mixed_record(ms, synth, dev, stream)
 
-    c4 = None
-    if args.c4 and rank == 0:
-        c4 = c4_record(ms, synth, dev, stream)
-
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -587,6 +619,28 @@ def main():
                "ms_per_step": el / args.e2e_steps * 1e3, "steps": args.e2e_steps,
                "timing": "host wall clock around synchronous C-ABI calls (pinned host buffers)"}
 
+    # ---- batched uneven workload (C4) and the 4-shank int16 run (C5), with the
+    # benchmark recording released first
+    c4 = c5 = None
+    if (args.c4 or args.c5) and rank == 0:
+        if "X" in locals():
+            del X
+        if "pre" in locals():
+            del pre
+        torch.cuda.empty_cache()
+        for flag, name, fn in ((args.c4, "c4", c4_record), (args.c5, "c5", c5_record)):
+            if not flag:
+                continue
+            try:
+                rec = fn(ms, synth, dev, stream)
+            except Exception as e:  # reported in the line; the headline fields stand
+                rec = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+            if name == "c4":
+                c4 = rec
+            else:
+                c5 = rec
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(M, N, cpu_threads())
@@ -605,6 +659,7 @@ def main():
             "step_roofline": step_roofline,
             "mixed": mixed,
             "batched_c4": c4,
+            "shanks_c5": c5,
             "cpu_baseline": cpu,
             "e2e": e2e,
         }
