@@ -482,6 +482,7 @@ int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* com
         if (components) c.finish(s);
         if (sigma) sg.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
+        whitening_check_timeout(s);
     });
 }
 

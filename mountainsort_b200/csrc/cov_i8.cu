@@ -610,6 +610,7 @@ void covariance_check_timeout(cudaStream_t stream) {
         MS3_CUDA(cudaStreamSynchronize(stream));
         throw Error(MS3GPU_ERR_CUDA, "tensor-core covariance: pipeline wait timed out");
     }
+    whitening_check_timeout(stream);
 }
 
 }  // namespace ms3gpu

@@ -99,6 +99,52 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void*
                  : "memory");
 }
 
+// ---- cluster shared memory
+
+// The shared::cluster address of the same shared-memory offset in CTA `rank`
+// of this cluster.
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+
+// 8-byte store into a cluster CTA's shared memory; its 8 bytes are counted on
+// that CTA's mbarrier `bar` (a shared::cluster address in the same CTA).
+__device__ __forceinline__ void st_async_b64(uint32_t addr, uint64_t v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(addr), "l"(v),
+                 "r"(bar)
+                 : "memory");
+}
+
+// try_wait with cluster-scope acquire: the stores of other CTAs that the
+// phase counted are visible once it returns true.
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait as mbar_wait, with cluster-scope acquire.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbar_try_wait_cluster(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        if (*reinterpret_cast<volatile int*>(err)) return false;
+        if (globaltimer_ns() - t0 > kTimeoutNs) {
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+
 __device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 // Waits until at most N bulk groups of this thread are still reading shared memory.

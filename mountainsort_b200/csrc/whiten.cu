@@ -32,6 +32,8 @@
 #include <string>
 
 #include "common.cuh"
+#include "ms3gpu.h"
+#include "tc_sm100.cuh"
 #include "whiten.h"
 
 namespace cg = cooperative_groups;
@@ -380,12 +382,20 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
 // the order pca_cluster forms it (per-lane column sums then the XOR
 // shuffle tree for a matvec row; 32-element warp trees summed in warp order
 // for a norm or a dot product), so components, sigma and W are identical.
-// Each warp forms the norm itself from the broadcast vector, so one
-// iteration is one matvec, one cluster barrier, the division and one block
-// barrier.  Matvec results alternate between two receive buffers: a CTA
-// writes buffer b of its peers only after every CTA has passed the barrier
-// that ended their reads of b.
+//
+// The matvec results are exchanged point to point instead of through a
+// cluster barrier: the warp that owns row m stores y[m] into every CTA's
+// receive buffer with st.async, whose bytes complete on the receiving CTA's
+// own mbarrier, and a CTA waits only for the M * 8 bytes of the step.  Step s
+// uses buffer s & 1 (phase s >> 1 of its mbarrier); a CTA writes buffer b of
+// step s + 2 only after it has received all of step s + 1, which every CTA
+// sends after its block barrier of step s, so nothing is overwritten while
+// it is read.  Each warp forms the norm itself from the received vector, so
+// one iteration is one matvec, one mbarrier wait, the division and one block
+// barrier.  Every wait is bounded (error flag g_pca_timeout).
 constexpr int kPcaWarps = kPcaThreads / 32;
+
+__device__ int g_pca_timeout;  // set when an exchange wait gave up (checked by the host)
 
 template <int RPW, int CPL>
 __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* __restrict__ XXt, int M,
@@ -395,12 +405,16 @@ __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* 
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int CS = (int)cluster.num_blocks();
+    int* err = &g_pca_timeout;
     __shared__ double ybuf[2][kMaxM];  // matvec results, written by every CTA
     __shared__ double vs[kMaxM];       // the normalised vector
     __shared__ double vinit[kMaxM];
     __shared__ double red[32];
+    __shared__ __align__(8) uint64_t ybar[2];  // bytes of ybuf[b] received in the current step
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const int row0 = (rank * kPcaWarps + w) * RPW;
+    const bool has_rows = row0 < M;
+    const uint32_t step_bytes = (uint32_t)M * 8u;
 
     double A[RPW][CPL];
 #pragma unroll
@@ -410,6 +424,11 @@ __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* 
             const int m = row0 + r, n = l + 32 * j;
             A[r][j] = (m < M && n < M) ? XXt[(size_t)m + (size_t)M * n] : 0.0;
         }
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&ybar[0], 1);
+        tc::mbar_init(&ybar[1], 1);
+        tc::fence_mbar_init();
+    }
     // start vector sin(i+1), normalised (pca.cpp:546-549, 457-466)
     for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = sin((double)(n + 1));
     __syncthreads();
@@ -421,72 +440,98 @@ __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* 
         if (nrm != 0.0)
             for (int n = threadIdx.x; n < M; n += blockDim.x) vinit[n] = vinit[n] / nrm;
     }
-    __syncthreads();
+    if (threadIdx.x == 0) {
+        tc::mbar_expect_tx(&ybar[0], step_bytes);  // steps 0 and 1
+        tc::mbar_expect_tx(&ybar[1], step_bytes);
+    }
+    // every CTA's barriers are initialised and armed before any store reaches them
+    cluster.sync();
+    // lane l < CS sends to CTA l: the cluster addresses of its buffers and barriers
+    const uint32_t rbuf = l < CS ? tc::mapa_shared(tc::smem_u32(&ybuf[0][0]), (uint32_t)l) : 0u;
+    const uint32_t rbar = l < CS ? tc::mapa_shared(tc::smem_u32(&ybar[0]), (uint32_t)l) : 0u;
 
-    // y = A v for this warp's rows, sent to every CTA's ybuf[b], then the barrier
-    auto matvec = [&](const double* v, int b) {
-        double s[RPW];
+    // y = A v for this warp's rows, stored into every CTA's ybuf[step & 1];
+    // then the wait for the whole vector of the step
+    auto matvec = [&](const double* v, int64_t step) -> bool {
+        const int b = (int)(step & 1);
+        if (has_rows) {
+            double s[RPW];
 #pragma unroll
-        for (int r = 0; r < RPW; r++) s[r] = 0.0;
+            for (int r = 0; r < RPW; r++) s[r] = 0.0;
 #pragma unroll
-        for (int j = 0; j < CPL; j++) {
-            const int n = l + 32 * j;
-            if (n < M) {
-                const double vn = v[n];
+            for (int j = 0; j < CPL; j++) {
+                const int n = l + 32 * j;
+                if (n < M) {
+                    const double vn = v[n];
 #pragma unroll
-                for (int r = 0; r < RPW; r++) s[r] += A[r][j] * vn;
+                    for (int r = 0; r < RPW; r++) s[r] += A[r][j] * vn;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RPW; r++) {
+                for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
+                const int m = row0 + r;
+                if (m < M && l < CS)
+                    tc::st_async_b64(rbuf + (uint32_t)((b * kMaxM + m) * 8), (uint64_t)__double_as_longlong(s[r]),
+                                     rbar + (uint32_t)(b * 8));
             }
         }
-#pragma unroll
-        for (int r = 0; r < RPW; r++) {
-            for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
-            const int m = row0 + r;
-            if (m < M)
-                for (int d = l; d < CS; d += 32) cluster.map_shared_rank(&ybuf[b][0], d)[m] = s[r];
-        }
-        cluster.sync();
+        const bool ok = tc::mbar_wait_cluster(&ybar[b], (uint32_t)((step >> 1) & 1), err);
+        // re-arm for step + 2: its stores arrive only after this CTA has sent step + 1
+        if (ok && threadIdx.x == 0) tc::mbar_expect_tx(&ybar[b], step_bytes);
+        return ok;
     };
 
-    int b = 0;  // receive buffer of the next matvec (same sequence in every CTA)
-    for (int k = 0; k < M; k++) {
+    int64_t step = 0;  // matvec count (same sequence in every CTA)
+    bool ok = true;
+    for (int k = 0; k < M && ok; k++) {
         const double* v = vinit;
         double sig = 0.0;
         for (int it = 0; it < num_iter; it++) {
-            matvec(v, b);
-            const double* y = ybuf[b];
-            sig = sqrt(warp_ordered_sum(M, [&](int n) { return y[n] * y[n]; }));
-            for (int n = threadIdx.x; n < M; n += blockDim.x) vs[n] = sig != 0.0 ? y[n] / sig : y[n];
-            __syncthreads();
+            const bool got = matvec(v, step);
+            const double* y = ybuf[step & 1];
+            if (got) {
+                sig = sqrt(warp_ordered_sum(M, [&](int n) { return y[n] * y[n]; }));
+                for (int n = threadIdx.x; n < M; n += blockDim.x) vs[n] = sig != 0.0 ? y[n] / sig : y[n];
+            }
+            ok = __syncthreads_and(got) != 0;
+            if (!ok) break;
             v = vs;
-            b ^= 1;
+            step++;
         }
+        if (!ok) break;
         if (rank == 0) {
             for (int n = threadIdx.x; n < M; n += blockDim.x) comps[(size_t)n + (size_t)M * k] = v[n];
             if (threadIdx.x == 0) sigma[k] = sig;
         }
         // deflation: X <- X - v u' - u v' + (v'u) v v',  u = X v
-        matvec(v, b);
-        const double* u = ybuf[b];
-        b ^= 1;
-        const double alpha = warp_ordered_sum(M, [&](int n) { return v[n] * u[n]; });
+        const bool got = matvec(v, step);
+        const double* u = ybuf[step & 1];
+        step++;
+        if (got && has_rows) {
+            const double alpha = warp_ordered_sum(M, [&](int n) { return v[n] * u[n]; });
 #pragma unroll
-        for (int r = 0; r < RPW; r++) {
-            const int m = row0 + r;
-            if (m >= M) continue;
-            const double vm = v[m], um = u[m];
+            for (int r = 0; r < RPW; r++) {
+                const int m = row0 + r;
+                if (m >= M) continue;
+                const double vm = v[m], um = u[m];
 #pragma unroll
-            for (int j = 0; j < CPL; j++) {
-                const int n = l + 32 * j;
-                if (n < M) {
-                    const double sdef = __dadd_rn(__dmul_rn(vm, u[n]), __dmul_rn(um, v[n]));
-                    const double x = __dsub_rn(A[r][j], sdef);
-                    A[r][j] = __dadd_rn(x, __dmul_rn(alpha, __dmul_rn(vm, v[n])));
+                for (int j = 0; j < CPL; j++) {
+                    const int n = l + 32 * j;
+                    if (n < M) {
+                        const double sdef = __dadd_rn(__dmul_rn(vm, u[n]), __dmul_rn(um, v[n]));
+                        const double x = __dsub_rn(A[r][j], sdef);
+                        A[r][j] = __dadd_rn(x, __dmul_rn(alpha, __dmul_rn(vm, v[n])));
+                    }
                 }
             }
         }
-        // vs is rewritten by the next component's first division only after
-        // its matvec's cluster barrier, which every thread reaches after this update
+        // vs and this buffer are read above; the next component rewrites vs
+        // after its first wait and the buffer two steps later
+        ok = __syncthreads_and(got) != 0;
     }
+    // no CTA leaves while a peer may still store into its shared memory
+    cluster.sync();
 }
 
 // W = (C D) C^T, D = diag(1/sqrt(sigma)) (0 where sigma == 0), in the
@@ -846,6 +891,18 @@ void whitening_matrix_device(const double* XXt, int64_t M, double* W, double* co
         MS3_CUDA(cudaFuncSetAttribute(w_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
     w_assemble<<<dim3((unsigned)ceil_div(M, 128), (unsigned)M), 128, wsm, stream>>>(comps, sigma, (int)M, W);
     MS3_LAUNCH_CHECK();
+}
+
+void whitening_check_timeout(cudaStream_t stream) {
+    int h = 0;
+    MS3_CUDA(cudaMemcpyFromSymbolAsync(&h, g_pca_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, stream));
+    MS3_CUDA(cudaStreamSynchronize(stream));
+    if (h) {
+        const int zero = 0;
+        MS3_CUDA(cudaMemcpyToSymbolAsync(g_pca_timeout, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, stream));
+        MS3_CUDA(cudaStreamSynchronize(stream));
+        throw Error(MS3GPU_ERR_CUDA, "power iteration: exchange wait timed out");
+    }
 }
 
 void pca_launch_smem(const double* XXt, int64_t M, double* comps, double* sigma, cudaStream_t stream) {

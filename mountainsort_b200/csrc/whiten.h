@@ -51,8 +51,12 @@ void cov_i8_partials(const float* X, int64_t M, int64_t r0, int64_t r1, int64_t 
                      cudaStream_t stream);
 void cov_i8_finish(const double* partials, int64_t runs, int64_t M, int64_t N, double* XXt, cudaStream_t stream);
 // Raises MS3GPU_ERR_CUDA (after a synchronize) when a tensor-core covariance
-// pipeline wait gave up, and clears the flag.
+// pipeline wait or a power-iteration exchange wait gave up, and clears the
+// flag.
 void covariance_check_timeout(cudaStream_t stream);
+
+// The power-iteration part of covariance_check_timeout.
+void whitening_check_timeout(cudaStream_t stream);
 
 // The same covariance with its partial sums in a fixed 16 MiB device array
 // instead of allocated scratch (X and XXt must be device memory).
