@@ -89,6 +89,14 @@ MS3GPU_API const char* ms3gpu_version(void);
  * throughput accounting; monotonically increasing). */
 MS3GPU_API uint64_t ms3gpu_launch_count(void);
 
+/* Device memory the library keeps for reuse between calls (its stream-ordered
+ * pool on the current device holds freed buffers instead of returning them)
+ * is handed back to the driver, after the work queued on the device has
+ * finished.  For callers that need that memory for something else between
+ * calls; the next call allocates again.  Not a replacement for any MountainSort
+ * interface (the reference's processors exit after each call). */
+MS3GPU_API int ms3gpu_release_cached_memory(void);
+
 /* The reference's chunk size for M channels and T threads
  * (p_bandpass_filter.cpp:147-155); the FFT length is chunk + 120000. */
 MS3GPU_API int64_t ms3gpu_bandpass_chunk_size(int64_t M, int32_t num_threads);

@@ -6,7 +6,8 @@ processor mirror, .mda I/O and the seeded synthetic-recording generator.
 """
 from . import mdaio  # noqa: F401
 from .api import (apply_whitening_matrix, bandpass_filter, bandpass_opts, bandpass_whiten,  # noqa: F401
-                  bandpass_whiten_batch, chunk_size, default_num_threads, requirements, whiten,
+                  bandpass_whiten_batch, chunk_size, default_num_threads, release_cached_memory,
+                  requirements, whiten,
                   whiten_blocks, whiten_covariance, whitening_matrix)
 from ._lib import Ms3GpuError  # noqa: F401
 

@@ -88,6 +88,7 @@ SIGNATURES = {
     "ms3gpu_last_error": (ctypes.c_char_p, []),
     "ms3gpu_version": (ctypes.c_char_p, []),
     "ms3gpu_launch_count": (ctypes.c_uint64, []),
+    "ms3gpu_release_cached_memory": (ctypes.c_int, []),
     "ms3gpu_bandpass_chunk_size": (_i64, [_i64, ctypes.c_int32]),
     "ms3gpu_bandpass_output_dims": (ctypes.c_int, [_i64, _i64, ctypes.POINTER(BandpassOpts),
                                                    ctypes.POINTER(_i64), ctypes.POINTER(_i64),

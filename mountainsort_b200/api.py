@@ -406,6 +406,13 @@ def whiten_clips(clips, W, quantization_unit=0.0, out=None, stream=None, precisi
     return out
 
 
+def release_cached_memory():
+    """Hands the device memory the library keeps between calls back to the
+    driver (ms3gpu_release_cached_memory), e.g. before allocating large
+    arrays with another allocator."""
+    check(_lib.load().ms3gpu_release_cached_memory())
+
+
 def requirements(processor: str, M: int, N: int, **params) -> float:
     """The processor's peak-RAM model in MB (its "requirements" answer)."""
     L = _lib.load()

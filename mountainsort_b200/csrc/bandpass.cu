@@ -1028,7 +1028,17 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
         MS3_CUDA(cudaGetDevice(&dev));
         MS3_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     }
-    DevBuf scratch((size_t)per_batch * unit_bytes, stream);
+    // fewer units per launch batch when the device has no room for the full scratch
+    DevBuf scratch;
+    for (;;) {
+        try {
+            scratch.alloc((size_t)per_batch * unit_bytes, stream);
+            break;
+        } catch (const Error& e) {
+            if (e.code != MS3GPU_ERR_NOMEM || per_batch == 1) throw;
+            per_batch = (per_batch + 1) / 2;
+        }
+    }
     const size_t fsm1 = ((size_t)plan->L1 * G + plan->L1) * sizeof(float2);
     const size_t fsm2 = ((size_t)plan->L2 * G + plan->L2) * sizeof(float2);
     // the register-pass inverse stores kept rows q in [4, 12) of each 16-point

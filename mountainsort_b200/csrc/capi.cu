@@ -6,6 +6,7 @@
 // the stream.  C++ exceptions never cross the boundary: they become status
 // codes plus the per-thread text returned by ms3gpu_last_error().
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -15,6 +16,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -162,6 +164,22 @@ struct OutView {
     }
 };
 
+// An NVTX range names each entry point on a profiler timeline (nvtx3 is
+// header-only: without a tool attached the calls return at once).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
+template <class F>
+int guarded(F&& f);
+
+template <class F>
+int guarded(const char* name, F&& f) {
+    NvtxRange range(name);
+    return guarded(std::forward<F>(f));
+}
+
 template <class F>
 int guarded(F&& f) {
     try {
@@ -231,6 +249,17 @@ const char* ms3gpu_version(void) { return "ms3gpu 0.1.0 (sm_100a)"; }
 
 uint64_t ms3gpu_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
+int ms3gpu_release_cached_memory(void) {
+    return guarded(__func__, [&] {
+        int dev = 0;
+        MS3_CUDA(cudaGetDevice(&dev));
+        cudaMemPool_t pool;
+        MS3_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        MS3_CUDA(cudaDeviceSynchronize());
+        MS3_CUDA(cudaMemPoolTrimTo(pool, 0));
+    });
+}
+
 int64_t ms3gpu_bandpass_chunk_size(int64_t M, int32_t num_threads) {
     if (M < 1 || num_threads < 1) return -1;
     return bandpass_chunk_size(M, num_threads);
@@ -238,7 +267,7 @@ int64_t ms3gpu_bandpass_chunk_size(int64_t M, int32_t num_threads) {
 
 int ms3gpu_bandpass_output_dims(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts, int64_t* M_out,
                                 int64_t* N_out, int32_t* dtype_out) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!opts) throw_invalid("opts is NULL");
         const int sub = opts->subsample_factor ? opts->subsample_factor : 1;
@@ -255,7 +284,7 @@ int ms3gpu_bandpass_output_dims(int64_t M, int64_t N, const ms3gpu_bandpass_opts
 }
 
 int ms3gpu_bandpass_requirements(int64_t M, int64_t N, const ms3gpu_bandpass_opts* opts, double* peak_ram_mb) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!opts || !peak_ram_mb) throw_invalid("NULL argument");
         if (opts->num_threads < 1) throw_invalid("num_threads must be >= 1");
@@ -268,7 +297,7 @@ int ms3gpu_bandpass_requirements(int64_t M, int64_t N, const ms3gpu_bandpass_opt
 }
 
 int ms3gpu_whiten_requirements(int64_t M, int64_t N, double* peak_ram_mb) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!peak_ram_mb) throw_invalid("NULL argument");
         // p_whiten.cpp:53-57
@@ -303,16 +332,71 @@ void bandpass_any(const void* timeseries, bool in_i16, int64_t M, int64_t N, voi
 
 int ms3gpu_bandpass_filter(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
                            const ms3gpu_bandpass_opts* opts, void* stream) {
-    return guarded([&] { bandpass_any(timeseries, false, M, N, timeseries_out, opts, stream); });
+    return guarded(__func__, [&] { bandpass_any(timeseries, false, M, N, timeseries_out, opts, stream); });
 }
 
 int ms3gpu_bandpass_filter_i16(const int16_t* timeseries, int64_t M, int64_t N, void* timeseries_out,
                                const ms3gpu_bandpass_opts* opts, void* stream) {
-    return guarded([&] { bandpass_any(timeseries, true, M, N, timeseries_out, opts, stream); });
+    return guarded(__func__, [&] { bandpass_any(timeseries, true, M, N, timeseries_out, opts, stream); });
 }
 
 namespace {
 // Device state of one batch job between its compute and its copy-back.
+// The filtered signal's device buffer for a filter + whiten call without a
+// caller filt buffer: a library buffer, or, when that does not fit beside the
+// caller's buffers and the output is float32, the output buffer itself
+// (in_place).  Returns nullptr with in_place set in that case.
+float* alloc_filt_or_in_place(size_t in_bytes, double q, DevBuf& filt_own, cudaStream_t s, bool& in_place) {
+    in_place = false;
+    if (!in_bytes) return nullptr;
+    const char* force = std::getenv("MS3GPU_FILT_IN_PLACE");  // testing: take the in-place path
+    if (force && force[0] == '1' && q <= 0) {
+        in_place = true;
+        return nullptr;
+    }
+    try {
+        filt_own.alloc(in_bytes, s);
+        return filt_own.as<float>();
+    } catch (const Error& e) {
+        if (e.code != MS3GPU_ERR_NOMEM || q > 0) throw;
+    }
+    in_place = true;
+    return nullptr;
+}
+
+// pre = W filt.  In place (filt_d is the float32 output buffer itself), the
+// output is whitened in time slabs of whole 128-row tiles through a 256 MiB
+// buffer and copied back: each output row depends only on its own filtered
+// row, so the values are those of the one-pass apply.
+void apply_maybe_in_place(const float* filt_d, bool in_place, int64_t M, int64_t N, const double* W, double q,
+                          bool mixed, void* pre_d, cudaStream_t s, int* err) {
+    if (!in_place) {
+        apply_whitening_device(filt_d, M, N, W, q, mixed, pre_d, s, err);
+        return;
+    }
+    const int64_t rows = std::max<int64_t>(128, (((int64_t)256 << 20) / (4 * std::max<int64_t>(1, M))) / 128 * 128);
+    DevBuf slab(sizeof(float) * (size_t)(std::min(rows, N) * M), s);
+    DevBuf own_err;
+    if (!err) {
+        own_err.alloc(sizeof(int), s);
+        MS3_CUDA(cudaMemsetAsync(own_err.get(), 0, sizeof(int), s));
+        err = own_err.as<int>();
+    }
+    float* pre_f = static_cast<float*>(pre_d);
+    for (int64_t r0 = 0; r0 < N; r0 += rows) {
+        const int64_t n = std::min(rows, N - r0);
+        apply_whitening_device(pre_f + r0 * M, M, n, W, q, mixed, slab.get(), s, err);
+        MS3_CUDA(cudaMemcpyAsync(pre_f + r0 * M, slab.get(), sizeof(float) * (size_t)(n * M), cudaMemcpyDeviceToDevice,
+                                 s));
+    }
+    if (own_err.get()) {
+        int herr = 0;
+        MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MS3_CUDA(cudaStreamSynchronize(s));
+        if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+    }
+}
+
 struct BatchJob {
     cudaStream_t s = nullptr;
     InView in;
@@ -336,15 +420,16 @@ void issue_batch_job(const ms3gpu_job& j, BatchJob& st) {
     cudaStream_t s = st.s;
     stage_in(st.in, j.timeseries, in_bytes, s);
     float* filt_d = nullptr;
+    bool in_place = false;
     if (j.filt_out) {
         st.filt.setup(j.filt_out, in_bytes, s);
         filt_d = static_cast<float*>(st.filt.ptr);
-    } else if (in_bytes) {
-        st.filt_own.alloc(in_bytes, s);
-        filt_d = st.filt_own.as<float>();
+    } else {
+        filt_d = alloc_filt_or_in_place(in_bytes, q, st.filt_own, s, in_place);
     }
-    bandpass_device(static_cast<const float*>(st.in.ptr), M, N, filt_d, p, s);
     st.pre.setup(j.pre_out, pre_bytes, s);
+    if (in_place) filt_d = static_cast<float*>(st.pre.ptr);
+    bandpass_device(static_cast<const float*>(st.in.ptr), M, N, filt_d, p, s);
     st.mats.alloc(sizeof(double) * (size_t)(2 * M * M), s);
     double* XXt = st.mats.as<double>();
     double* W = XXt + M * M;
@@ -352,7 +437,7 @@ void issue_batch_job(const ms3gpu_job& j, BatchJob& st) {
     whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
     st.err.alloc(sizeof(int), s);
     MS3_CUDA(cudaMemsetAsync(st.err.get(), 0, sizeof(int), s));
-    apply_whitening_device(filt_d, M, N, W, q, mixed, st.pre.ptr, s, st.err.as<int>());
+    apply_maybe_in_place(filt_d, in_place, M, N, W, q, mixed, st.pre.ptr, s, st.err.as<int>());
 }
 }  // namespace
 
@@ -364,7 +449,15 @@ int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream)
         require(jobs, "jobs", n_jobs > 0);
         if (n_jobs == 0) return;
         cudaStream_t s0 = as_stream(stream);
-        const int K = std::min<int>(n_jobs, 4);
+        // Jobs of at least `large` ch-samples (default 3e8, 384 channels x 26 s)
+        // fill the GPU by themselves (their persistent kernels take one CTA per
+        // SM): they run one after another on the first stream, before the
+        // smaller jobs, which are spread over K streams so that their short and
+        // latency-bound kernels overlap.
+        const char* ks = std::getenv("MS3GPU_BATCH_STREAMS");
+        const char* ls = std::getenv("MS3GPU_BATCH_LARGE");
+        const int K = std::max(1, std::min<int>(n_jobs, (ks && *ks) ? std::atoi(ks) : 4));
+        const double large = (ls && *ls) ? std::atof(ls) : 3e8;
         std::vector<cudaStream_t> streams((size_t)K, nullptr);
         cudaEvent_t start = nullptr;
         MS3_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
@@ -382,9 +475,22 @@ int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream)
             }
         };
         // phase 1: every job's device work, round-robin over the streams
-        for (int i = 0; i < n_jobs; i++) {
+        std::vector<int> order;
+        for (int i = 0; i < n_jobs; i++)
+            if ((double)jobs[i].M * (double)jobs[i].N >= large) order.push_back(i);
+        const size_t nlarge = order.size();
+        for (int i = 0; i < n_jobs; i++)
+            if ((double)jobs[i].M * (double)jobs[i].N < large) order.push_back(i);
+        cudaEvent_t large_done = nullptr;
+        for (size_t k = 0; k < order.size(); k++) {
+            const int i = order[k];
+            if (k == nlarge && nlarge > 0) {  // the small jobs start once the large ones are done
+                MS3_CUDA(cudaEventCreateWithFlags(&large_done, cudaEventDisableTiming));
+                MS3_CUDA(cudaEventRecord(large_done, streams[0]));
+                for (int t = 1; t < K; t++) MS3_CUDA(cudaStreamWaitEvent(streams[(size_t)t], large_done, 0));
+            }
             state[(size_t)i].reset(new BatchJob);
-            state[(size_t)i]->s = streams[(size_t)(i % K)];
+            state[(size_t)i]->s = streams[k < nlarge ? 0 : (size_t)((k - nlarge) % K)];
             jobs[i].status = MS3GPU_OK;
             const int code = guarded([&] { issue_batch_job(jobs[i], *state[(size_t)i]); });
             if (code != MS3GPU_OK) record(i, code, ms3gpu_last_error());
@@ -415,6 +521,7 @@ int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream)
             MS3_CUDA(cudaStreamDestroy(st));
         }
         MS3_CUDA(cudaEventDestroy(start));
+        if (large_done) MS3_CUDA(cudaEventDestroy(large_done));
         bandpass_check_timeout(s0);
         covariance_check_timeout(s0);
     });
@@ -427,7 +534,7 @@ int ms3gpu_bandpass_whiten_batch(ms3gpu_job* jobs, int32_t n_jobs, void* stream)
 }
 
 int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, double* XXt, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         cudaStream_t s = as_stream(stream);
         const size_t in_bytes = sizeof(float) * (size_t)(M * N);
@@ -446,7 +553,7 @@ int ms3gpu_whiten_covariance(const float* timeseries, int64_t M, int64_t N, doub
 
 int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t N, double* XXt,
                                      void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         cudaStream_t s = as_stream(stream);
         require(timeseries, "timeseries", M * N > 0);
@@ -463,7 +570,7 @@ int ms3gpu_whiten_covariance_noalloc(const float* timeseries, int64_t M, int64_t
 
 int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* components, double* sigma,
                             void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, 0);
         cudaStream_t s = as_stream(stream);
         const size_t mm = sizeof(double) * (size_t)(M * M);
@@ -489,7 +596,7 @@ int ms3gpu_whitening_matrix(const double* XXt, int64_t M, double* W, double* com
 int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N, const double* W,
                                   double quantization_unit, int32_t precision, void* timeseries_out,
                                   void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         cudaStream_t s = as_stream(stream);
         const size_t in_bytes = sizeof(float) * (size_t)(M * N);
@@ -512,7 +619,7 @@ int ms3gpu_apply_whitening_matrix(const float* timeseries, int64_t M, int64_t N,
 int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const int64_t* N_list, int32_t n_inputs,
                                     int64_t M, const int32_t* channels, int32_t n_channels, double* W_out,
                                     void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (n_inputs < 1) throw_invalid("timeseries_list is empty");
         require(timeseries_list, "timeseries_list", true);
         require(N_list, "N_list", true);
@@ -577,7 +684,7 @@ int ms3gpu_compute_whitening_matrix(const float* const* timeseries_list, const i
 int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const int32_t* channels,
                          const int32_t* block_sizes, int32_t n_blocks, void* timeseries_out,
                          const ms3gpu_whiten_opts* opts, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!opts) throw_invalid("whiten opts is NULL");
         if (n_blocks < 1) throw_invalid("n_blocks must be positive");
@@ -639,7 +746,7 @@ int ms3gpu_whiten_blocks(const float* timeseries, int64_t M, int64_t N, const in
 int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int64_t N, double threshold,
                               int64_t interval_size, float* timeseries_out, int64_t* timepoints_kept,
                               void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         // p_mask_out_artifacts.cpp:26-29
         if (threshold == 0 || interval_size <= 0)
@@ -663,7 +770,7 @@ int ms3gpu_mask_out_artifacts(const float* timeseries, int64_t M, int64_t N, dou
 int ms3gpu_detect_events(const float* timeseries, int64_t M, int64_t N, double detect_threshold,
                          double detect_interval, int32_t detect_sign, int64_t chunk_size, int64_t* counts,
                          int64_t* times, int64_t capacity, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         require(counts, "counts", M > 0);
         cudaStream_t s = as_stream(stream);
@@ -686,7 +793,7 @@ int ms3gpu_detect_events(const float* timeseries, int64_t M, int64_t N, double d
 
 int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, const double* W,
                         double quantization_unit, int32_t precision, void* clips_out, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         if (T < 0 || L < 0) throw_invalid("negative dimension");
         if (T > 0 && L > std::numeric_limits<int64_t>::max() / T) throw_invalid("clips too large");
         const int64_t N = T * L;
@@ -713,7 +820,7 @@ int ms3gpu_whiten_clips(const float* clips, int64_t M, int64_t T, int64_t L, con
 
 int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeseries_out,
                   const ms3gpu_whiten_opts* opts, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!opts) throw_invalid("whiten opts is NULL");
         cudaStream_t s = as_stream(stream);
@@ -741,7 +848,7 @@ int ms3gpu_whiten(const float* timeseries, int64_t M, int64_t N, void* timeserie
 
 int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float* filt_out, void* pre_out,
                            const ms3gpu_bandpass_opts* bp, const ms3gpu_whiten_opts* wh, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         BandpassParams p = to_params(bp);
         if (!wh) throw_invalid("whiten opts is NULL");
@@ -765,23 +872,27 @@ int ms3gpu_bandpass_whiten(const float* timeseries, int64_t M, int64_t N, float*
         OutView filt;
         DevBuf filt_own;
         float* filt_d = nullptr;
+        bool in_place = false;
         if (filt_out) {
             filt.setup(filt_out, in_bytes, s);
             filt_d = static_cast<float*>(filt.ptr);
-        } else if (in_bytes) {
-            filt_own.alloc(in_bytes, s);
-            filt_d = filt_own.as<float>();
+        } else {
+            filt_d = alloc_filt_or_in_place(in_bytes, q, filt_own, s, in_place);
+        }
+        OutView pre;
+        if (in_place) {  // the filtered signal goes into the output buffer (never the staged input)
+            pre.setup(pre_out, pre_bytes, s);
+            filt_d = static_cast<float*>(pre.ptr);
         }
         bandpass_device(static_cast<const float*>(in.ptr), M, N, filt_d, p, s);
         // The staged raw input is dead once filtered: the whitened output may reuse it.
-        OutView pre;
-        pre.setup(pre_out, pre_bytes, s, &in.own);
+        if (!in_place) pre.setup(pre_out, pre_bytes, s, &in.own);
         DevBuf mats(sizeof(double) * (size_t)(2 * M * M), s);
         double* XXt = mats.as<double>();
         double* W = XXt + M * M;
         covariance_device(filt_d, M, N, XXt, s);
         whitening_matrix_device(XXt, M, W, nullptr, nullptr, s);
-        apply_whitening_device(filt_d, M, N, W, q, check_precision(wh->precision), pre.ptr, s);
+        apply_maybe_in_place(filt_d, in_place, M, N, W, q, check_precision(wh->precision), pre.ptr, s, nullptr);
         if (filt_out) filt.finish(s);
         pre.finish(s);
         MS3_CUDA(cudaStreamSynchronize(s));
@@ -794,7 +905,7 @@ int ms3gpu_bandpass_filter_windows(const void* timeseries, int32_t in_dtype, int
                                    int64_t rows, int64_t c_begin, int64_t c_end, void* timeseries_out,
                                    int64_t out_row0, int64_t out_rows, const ms3gpu_bandpass_opts* opts,
                                    void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         BandpassParams p = to_params(opts);
         if (in_dtype != MS3GPU_DTYPE_FLOAT32 && in_dtype != MS3GPU_DTYPE_INT16)
@@ -839,7 +950,7 @@ int ms3gpu_bandpass_filter_windows(const void* timeseries, int32_t in_dtype, int
 }
 
 int ms3gpu_whiten_covariance_sum(const float* timeseries, int64_t M, int64_t N, double* XXt_sum, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         require(XXt_sum, "XXt_sum", M > 0);
         cudaStream_t s = as_stream(stream);
@@ -871,7 +982,7 @@ void check_stream_io(const ms3gpu_stream_io* io, bool needs_write) {
 
 int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dtype, const ms3gpu_stream_io* io,
                                   const ms3gpu_bandpass_opts* opts, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         BandpassParams p = to_params(opts);
         check_stream_io(io, true);
@@ -883,7 +994,7 @@ int ms3gpu_bandpass_filter_stream(int64_t M, int64_t N, int32_t in_dtype, const 
 
 int ms3gpu_mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int64_t interval_size,
                                      const ms3gpu_stream_io* io, int64_t* timepoints_kept, void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (threshold == 0 || interval_size <= 0)
             throw_invalid("Problem with input parameters. Either threshold or interval_size is zero.");
@@ -895,7 +1006,7 @@ int ms3gpu_mask_out_artifacts_stream(int64_t M, int64_t N, double threshold, int
 
 int ms3gpu_whiten_stream(int64_t M, int64_t N, const ms3gpu_stream_io* io, const ms3gpu_whiten_opts* opts,
                          void* stream) {
-    return guarded([&] {
+    return guarded(__func__, [&] {
         check_shape(M, N);
         if (!opts) throw_invalid("whiten opts is NULL");
         check_stream_io(io, true);

@@ -69,6 +69,7 @@ constexpr int kPlaneStage = 2 * 4 * kPlaneBytes;
 constexpr int kConvWarps = 16;
 constexpr int kThreads = (2 + kConvWarps + 4) * 32;  // 704
 static_assert(kKT == 2 * kConvWarps, "each converter thread takes two rows of a stage");
+static_assert(kS1 == kS2, "the converters walk both rings with one stage counter");
 constexpr int kSentinel = 1000;               // scale exponent of a channel whose run holds inf / NaN
 constexpr size_t kSmemBytes = (size_t)kS1 * kF32Stage + (size_t)kS2 * kPlaneStage + 2 * kB * sizeof(int) +
                               1024 /*align*/ + 256 /*barriers*/;
@@ -314,13 +315,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         if (lane == 0) {
             int64_t g = 0;
+            int gs = 0;        // g % kS1
+            uint32_t gph = 0;  // (g / kS1) & 1
             bool ok = true;
             for (int64_t i = 0; i < my_items && ok; i++) {
                 const Item it = item_of(i);
                 const bool diag = it.bi == it.bj;
                 for (int kb = 0; kb < it.nkb; kb++, g++) {
-                    const int s = (int)(g % kS1);
-                    if (g >= kS1 && !(ok = tc::mbar_wait(&f_empty[s], (uint32_t)(((g / kS1) - 1) & 1), err))) break;
+                    const int s = gs;
+                    if (g >= kS1 && !(ok = tc::mbar_wait(&f_empty[s], gph ^ 1u, err))) break;
+                    if (++gs == kS1) {
+                        gs = 0;
+                        gph ^= 1u;
+                    }
                     uint8_t* dst = f32 + (size_t)s * kF32Stage;
                     const int y = (int)(it.r * R + (int64_t)kb * kKT);
                     tc::mbar_expect_tx(&f_full[s], diag ? kF32Bytes : 2 * kF32Bytes);
@@ -335,6 +342,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             int64_t g = 0;
+            int gs = 0;        // g % kS2
+            uint32_t gph = 0;  // (g / kS2) & 1
             bool ok = true;
             for (int64_t i = 0; i < my_items && ok; i++) {
                 const Item it = item_of(i);
@@ -342,8 +351,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (i > 0 && !(ok = tc::mbar_wait(acc_free, (uint32_t)((i - 1) & 1), err))) break;
                 tc::tc_fence_after();
                 for (int kb = 0; kb < it.nkb; kb++, g++) {
-                    const int s = (int)(g % kS2);
-                    if (!(ok = tc::mbar_wait(&p_full[s], (uint32_t)((g / kS2) & 1), err))) break;
+                    const int s = gs;
+                    if (!(ok = tc::mbar_wait(&p_full[s], gph, err))) break;
+                    if (++gs == kS2) {
+                        gs = 0;
+                        gph ^= 1u;
+                    }
                     tc::tc_fence_after();
                     const uint32_t pa = tc::smem_u32(planes + (size_t)s * kPlaneStage);
                     const uint32_t pb = diag ? pa : pa + 4 * kPlaneBytes;
@@ -377,6 +390,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = tid & 31;   // channel quad within a block: channels 4q .. 4q+3
         const int tg = tid >> 5;  // rows tg and tg + 16 of each stage
         int64_t g = 0;
+        int gs = 0;         // g % kS1 (= g % kS2)
+        uint32_t gph = 0;   // (g / kS1) & 1
         bool ok = true;
         for (int64_t i = 0; i < my_items && ok; i++) {
             const Item it = item_of(i);
@@ -395,12 +410,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             int dsum[4] = {0, 0, 0, 0};  // sums of d2^2 per channel (diagonal items)
             for (int kb = 0; kb < it.nkb; kb++, g++) {
-                const int s1 = (int)(g % kS1), s2 = (int)(g % kS2);
-                ok = tc::mbar_wait(&f_full[s1], (uint32_t)((g / kS1) & 1), err);
-                if (ok && g >= kS2) ok = tc::mbar_wait(&p_empty[s2], (uint32_t)(((g / kS2) - 1) & 1), err);
+                const int s1 = gs, s2 = gs;
+                ok = tc::mbar_wait(&f_full[s1], gph, err);
+                if (ok && g >= kS2) ok = tc::mbar_wait(&p_empty[s2], gph ^ 1u, err);
                 if (!__all_sync(0xffffffffu, ok)) {
                     ok = false;
                     break;
+                }
+                if (++gs == kS1) {  // stage and phase of K-block g + 1
+                    gs = 0;
+                    gph ^= 1u;
                 }
                 const uint8_t* src = f32 + (size_t)s1 * kF32Stage;
                 uint8_t* dst = planes + (size_t)s2 * kPlaneStage;

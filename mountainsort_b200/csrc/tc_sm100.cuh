@@ -57,13 +57,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// try_wait that may suspend the thread until the phase completes, for at
+// most kSuspendNs: a waiting warp then takes no issue slots from the warps
+// doing the work.
+constexpr uint32_t kSuspendNs = 1000000;  // 1 ms
+
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait for the phase with the given parity.  Returns false (and sets
-// *err) on timeout or when another thread has already failed.
+// *err) on timeout or when another thread has already failed.  The flag and
+// the clock are read once per eight suspending probes.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
-        if (mbar_try_wait(bar, parity)) return true;
+#pragma unroll 1
+        for (int k = 0; k < 8; k++)
+            if (mbar_try_wait_suspend(bar, parity)) return true;
         if (*reinterpret_cast<volatile int*>(err)) return false;
         if (globaltimer_ns() - t0 > kTimeoutNs) {
             atomicExch(err, 1);
@@ -131,12 +151,26 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t pa
     return ok != 0;
 }
 
+__device__ __forceinline__ bool mbar_try_wait_cluster_suspend(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait as mbar_wait, with cluster-scope acquire.
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, int* err) {
     if (mbar_try_wait_cluster(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
-        if (mbar_try_wait_cluster(bar, parity)) return true;
+#pragma unroll 1
+        for (int k = 0; k < 8; k++)
+            if (mbar_try_wait_cluster_suspend(bar, parity)) return true;
         if (*reinterpret_cast<volatile int*>(err)) return false;
         if (globaltimer_ns() - t0 > kTimeoutNs) {
             atomicExch(err, 1);

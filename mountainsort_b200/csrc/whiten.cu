@@ -386,14 +386,19 @@ __global__ void __launch_bounds__(kPcaThreads) pca_cluster(const double* __restr
 // The matvec results are exchanged point to point instead of through a
 // cluster barrier: the warp that owns row m stores y[m] into every CTA's
 // receive buffer with st.async, whose bytes complete on the receiving CTA's
-// own mbarrier, and a CTA waits only for the M * 8 bytes of the step.  Step s
-// uses buffer s & 1 (phase s >> 1 of its mbarrier); a CTA writes buffer b of
-// step s + 2 only after it has received all of step s + 1, which every CTA
-// sends after its block barrier of step s, so nothing is overwritten while
-// it is read.  Each warp forms the norm itself from the received vector, so
-// one iteration is one matvec, one mbarrier wait, the division and one block
-// barrier.  Every wait is bounded (error flag g_pca_timeout).
+// own mbarrier.  Every CTA also sends every CTA (itself included) an 8-byte
+// token per step, so a CTA waits for (M + CS) * 8 bytes: the tokens make
+// each step depend on every CTA having finished the previous one, also for
+// CTAs that own no rows (small M).  Step s uses buffer s & 1 (phase s >> 1
+// of its mbarrier); a CTA sends step s + 2 only after it has received all of
+// step s + 1, and every CTA sends step s + 1 after its block barrier of step
+// s, so no buffer is overwritten while it is read and no CTA's mbarrier gets
+// two phases ahead of one of its threads.  Each warp forms the norm itself
+// from the received vector, so one iteration is one matvec, one mbarrier
+// wait, the division and one block barrier.  Every wait is bounded (error
+// flag g_pca_timeout).
 constexpr int kPcaWarps = kPcaThreads / 32;
+constexpr int kPcaMaxCluster = 16;  // token slots; the register kernel runs in clusters of 8
 
 __device__ int g_pca_timeout;  // set when an exchange wait gave up (checked by the host)
 
@@ -411,10 +416,11 @@ __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* 
     __shared__ double vinit[kMaxM];
     __shared__ double red[32];
     __shared__ __align__(8) uint64_t ybar[2];  // bytes of ybuf[b] received in the current step
+    __shared__ __align__(8) uint64_t tok[2][kPcaMaxCluster];  // one token per sending CTA and step
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const int row0 = (rank * kPcaWarps + w) * RPW;
     const bool has_rows = row0 < M;
-    const uint32_t step_bytes = (uint32_t)M * 8u;
+    const uint32_t step_bytes = (uint32_t)(M + CS) * 8u;
 
     double A[RPW][CPL];
 #pragma unroll
@@ -449,11 +455,14 @@ __global__ void __launch_bounds__(kPcaThreads, 1) pca_cluster_reg(const double* 
     // lane l < CS sends to CTA l: the cluster addresses of its buffers and barriers
     const uint32_t rbuf = l < CS ? tc::mapa_shared(tc::smem_u32(&ybuf[0][0]), (uint32_t)l) : 0u;
     const uint32_t rbar = l < CS ? tc::mapa_shared(tc::smem_u32(&ybar[0]), (uint32_t)l) : 0u;
+    const uint32_t rtok = l < CS ? tc::mapa_shared(tc::smem_u32(&tok[0][0]), (uint32_t)l) : 0u;
 
     // y = A v for this warp's rows, stored into every CTA's ybuf[step & 1];
     // then the wait for the whole vector of the step
     auto matvec = [&](const double* v, int64_t step) -> bool {
         const int b = (int)(step & 1);
+        if (w == 0 && l < CS)
+            tc::st_async_b64(rtok + (uint32_t)((b * kPcaMaxCluster + rank) * 8), 0ull, rbar + (uint32_t)(b * 8));
         if (has_rows) {
             double s[RPW];
 #pragma unroll

@@ -65,3 +65,48 @@ def test_batch_failing_job_is_isolated(gpu_lib):
     for k in (0, 2):
         assert np.all(np.isfinite(outs[k]))
     assert np.all(np.isnan(outs[1]))
+
+
+def test_filtered_signal_in_the_output_buffer_gives_the_same_values(gpu_lib, monkeypatch):
+    """When the library's filtered-signal buffer does not fit beside the
+    caller's buffers, a float32 output buffer holds the filtered signal and
+    is whitened in place in slabs (forced here with MS3GPU_FILT_IN_PLACE):
+    the outputs must be those of the ordinary path, for single calls on
+    device buffers and for a batch."""
+    import torch
+
+    recs = _recordings()[2:]
+    dev = torch.device("cuda", 0)
+    base = []
+    for r in recs:
+        Xd = torch.from_numpy(r["X"]).to(dev)
+        base.append(api.bandpass_whiten(Xd, r["samplerate"], r["freq_min"], r["freq_max"],
+                                        num_threads=r["num_threads"]).cpu().numpy())
+    base_batch = api.bandpass_whiten_batch(recs)
+    monkeypatch.setenv("MS3GPU_FILT_IN_PLACE", "1")
+    for k, r in enumerate(recs):
+        Xd = torch.from_numpy(r["X"]).to(dev)
+        got = api.bandpass_whiten(Xd, r["samplerate"], r["freq_min"], r["freq_max"],
+                                  num_threads=r["num_threads"]).cpu().numpy()
+        np.testing.assert_array_equal(got, base[k], err_msg=f"single {k}")
+    for k, (got, want) in enumerate(zip(api.bandpass_whiten_batch(recs), base_batch)):
+        np.testing.assert_array_equal(got, want, err_msg=f"batch job {k}")
+
+
+def test_many_small_recordings_in_one_batch(gpu_lib):
+    """24 short recordings of 16-100 channels in one batch: their power
+    iterations run concurrently on the batch's streams with most CTAs of each
+    cluster owning no rows.  Every job must succeed and equal its single
+    call bit for bit."""
+    rng = np.random.default_rng(7)
+    recs = []
+    for k in range(24):
+        M = int([16, 32, 40, 64, 100][k % 5])
+        N = int(rng.integers(130_000, 250_000))
+        recs.append(dict(X=synth.generate_numpy(M, N, K=4, seed=300 + k), samplerate=30000.0, freq_min=300.0,
+                         freq_max=6000.0, num_threads=16))
+    outs = api.bandpass_whiten_batch(recs)
+    for k, (r, out) in enumerate(zip(recs, outs)):
+        single = api.bandpass_whiten(r["X"], r["samplerate"], r["freq_min"], r["freq_max"],
+                                     num_threads=r["num_threads"])
+        np.testing.assert_array_equal(out, single, err_msg=f"job {k}")
