@@ -455,13 +455,18 @@ __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scra
 
 // F2, pipelined: the same arithmetic as bpr_rows_filter (bit-identical
 // results) in a persistent CTA per SM that walks rows r = blockIdx.x +
-// j * gridDim.x.  Each row (L2 x 16 complex values, 64000 bytes), its twiddle
-// row and its kernel row arrive by 1-D bulk copies into a ring of kF2Ring
-// shared-memory slots, issued kF2Ring rows ahead, so the global-load latency
-// overlaps the previous rows' arithmetic.  The three register passes then run
-// in place in the slot; the result goes straight back to the scratch row.
-constexpr int kF2Ring = 3;
-constexpr int kF2Threads = 416;  // 400 items in the outer passes, 320 in the middle one
+// j * gridDim.x.  A copy warp brings each row (L2 x 16 complex values, 64000
+// bytes), its twiddle row and its kernel row by 1-D bulk copies into a ring
+// of kF2Ring shared-memory slots, one row ahead of the compute warps, and
+// refills a slot as soon as the 13 compute warps have released it.  The three
+// register passes ping-pong between the slot and one transfer buffer (slot ->
+// transfer -> slot), so a row needs only two barriers of the compute warps
+// (named barrier 1): one after each exchange.  A failed wait sets the error
+// flag; the warps keep the same barrier sequence (skipping their stores), so
+// the kernel still ends.
+constexpr int kF2Ring = 2;
+constexpr int kF2Compute = 416;              // 400 items in the outer passes, 320 in the middle one
+constexpr int kF2Threads = kF2Compute + 32;  // and the copy warp
 
 __device__ int g_bp_timeout;  // set when a pipeline wait gave up (checked by the host)
 
@@ -473,10 +478,14 @@ struct F2Pipe {
     static constexpr int kTwBytes = n * 8;
     static constexpr int kKernBytes = n * 8;  // (hi, lo) per bin
     static constexpr int kSlotBytes = kRowBytes + kTwBytes + kKernBytes;
-    static constexpr size_t kSmemBytes = (size_t)kF2Ring * kSlotBytes + n * 8 + kF2Ring * 8;
+    static constexpr size_t kSmemBytes =
+        (size_t)kF2Ring * kSlotBytes + kRowBytes /*transfer*/ + n * 8 /*roots*/ + 2 * kF2Ring * 8 /*barriers*/;
     static_assert(kRowBytes % 16 == 0 && kTwBytes % 16 == 0 && kKernBytes % 16 == 0, "bulk copies need 16-byte sizes");
-    static_assert(SB * G <= kF2Threads && SA * G <= kF2Threads, "one item per thread");
+    static_assert(SB * G <= kF2Compute && SA * G <= kF2Compute, "one item per thread");
 };
+
+// Named barrier 1 over the compute warps of the row pass.
+__device__ __forceinline__ void f2_compute_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kF2Compute) : "memory"); }
 
 template <int SA, int SB>
 __global__ void __launch_bounds__(kF2Threads, 1)
@@ -486,8 +495,11 @@ __global__ void __launch_bounds__(kF2Threads, 1)
     constexpr int n = P::n, G = P::G;
     extern __shared__ float4 smem_f4[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(smem_f4);
-    float2* rt = reinterpret_cast<float2*>(smem + (size_t)kF2Ring * P::kSlotBytes);
+    float2* xfer = reinterpret_cast<float2*>(smem + (size_t)kF2Ring * P::kSlotBytes);
+    float2* rt = xfer + n * G;
     uint64_t* full = reinterpret_cast<uint64_t*>(rt + n);
+    uint64_t* empty = full + kF2Ring;
+    int* err = &g_bp_timeout;
     const int64_t L1 = g.L1;
     const int64_t mine = (blockIdx.x < nrows) ? (nrows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     auto slot_ptr = [&](int64_t j) { return smem + (size_t)(j % kF2Ring) * P::kSlotBytes; };
@@ -495,26 +507,43 @@ __global__ void __launch_bounds__(kF2Threads, 1)
         const int64_t r = blockIdx.x + j * gridDim.x;
         return scratch + (size_t)(r / L1) * (size_t)(g.L * G) + (size_t)(r % L1) * (n * G);
     };
-    auto issue = [&](int64_t j) {
-        const int64_t k1 = (blockIdx.x + j * gridDim.x) % L1;
-        uint8_t* slot = slot_ptr(j);
-        uint64_t* bar = &full[j % kF2Ring];
-        tc::mbar_expect_tx(bar, P::kSlotBytes);
-        tc::bulk_load_1d(slot, row_ptr(j), P::kRowBytes, bar);
-        tc::bulk_load_1d(slot + P::kRowBytes, twL + k1 * n, P::kTwBytes, bar);
-        tc::bulk_load_1d(slot + P::kRowBytes + P::kTwBytes, kern + k1 * n, P::kKernBytes, bar);
-    };
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kF2Ring; s++) tc::mbar_init(&full[s], 1);
+        for (int s = 0; s < kF2Ring; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], kF2Compute / 32);
+        }
         tc::fence_mbar_init();
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
     __syncthreads();
-    if (threadIdx.x == 0)
-        for (int64_t j = 0; j < mine && j < kF2Ring; j++) issue(j);
+
+    if (threadIdx.x >= kF2Compute) {
+        // the copy warp: row j into slot j % kF2Ring once its previous row is released
+        if (threadIdx.x == kF2Compute) {
+            int64_t issued = 0;
+            for (int64_t j = 0; j < mine; j++) {
+                if (j >= kF2Ring &&
+                    !tc::mbar_wait(&empty[j % kF2Ring], (uint32_t)(((j / kF2Ring) - 1) & 1), err))
+                    break;
+                const int64_t k1 = (blockIdx.x + j * gridDim.x) % L1;
+                uint8_t* slot = slot_ptr(j);
+                uint64_t* bar = &full[j % kF2Ring];
+                tc::mbar_expect_tx(bar, P::kSlotBytes);
+                tc::bulk_load_1d(slot, row_ptr(j), P::kRowBytes, bar);
+                tc::bulk_load_1d(slot + P::kRowBytes, twL + k1 * n, P::kTwBytes, bar);
+                tc::bulk_load_1d(slot + P::kRowBytes + P::kTwBytes, kern + k1 * n, P::kKernBytes, bar);
+                issued = j + 1;
+            }
+            // no copy may still be landing in shared memory when the CTA exits
+            for (int64_t j = (issued > kF2Ring ? issued - kF2Ring : 0); j < issued; j++)
+                tc::mbar_wait(&full[j % kF2Ring], (uint32_t)((j / kF2Ring) & 1), err);
+        }
+        return;
+    }
 
     const int t = threadIdx.x;
     const bool outer = t < SB * G, middle = t < SA * G;
+    bool ok = true;
     for (int64_t j = 0; j < mine; j++) {
         // Re-derived every row through an opaque move: otherwise the compiler
         // keeps the 40-odd loop-invariant root offsets q * i in registers
@@ -522,50 +551,43 @@ __global__ void __launch_bounds__(kF2Threads, 1)
         int i;
         asm volatile("shr.b32 %0, %1, 4;" : "=r"(i) : "r"(t));
         const int gi = t & (G - 1);
-        const bool landed = tc::mbar_wait(&full[j % kF2Ring], (uint32_t)((j / kF2Ring) & 1), &g_bp_timeout);
-        if (!__syncthreads_and(landed)) break;
+        if (ok) ok = tc::mbar_wait(&full[j % kF2Ring], (uint32_t)((j / kF2Ring) & 1), err);
         uint8_t* slot = slot_ptr(j);
         float2* buf = reinterpret_cast<float2*>(slot);
         const float2* tw = reinterpret_cast<const float2*>(slot + P::kRowBytes);
         const float2* kr = reinterpret_cast<const float2*>(slot + P::kRowBytes + P::kTwBytes);
-        // forward pass 1 (radix SA over items i < SB), in place
-        float2 u[SA];
+        // forward pass 1 (radix SA over items i < SB): slot -> transfer buffer
         if (outer) {
+            float2 u[SA];
 #pragma unroll
             for (int q = 0; q < SA; q++) {
                 const int n2 = i + q * SB;
                 u[q] = cmul(buf[n2 * G + gi], tw[n2]);
             }
             RegDft<SA, false>::run(u);
-        }
-        __syncthreads();
-        if (outer) {
 #pragma unroll
-            for (int q = 0; q < SA; q++) buf[(i * SA + q) * G + gi] = u[q];
+            for (int q = 0; q < SA; q++) xfer[(i * SA + q) * G + gi] = u[q];
         }
-        __syncthreads();
-        // forward pass 2 (radix SB, items i < SA), kernel, inverse pass 1
-        float2 v[SB];
+        f2_compute_bar();
+        // forward pass 2 (radix SB, items i < SA), kernel, inverse pass 1: transfer -> slot
         if (middle) {
+            float2 v[SB];
 #pragma unroll
             for (int q = 0; q < SB; q++) {
-                const float2 x = buf[(i + q * SA) * G + gi];
+                const float2 x = xfer[(i + q * SA) * G + gi];
                 v[q] = (q == 0) ? x : cmul(x, rt[q * i]);
             }
             RegDft<SB, false>::run(v);
 #pragma unroll
             for (int q = 0; q < SB; q++) v[q] = kern_mul(v[q], kr[i + q * SA]);
             RegDft<SB, true>::run(v);
-        }
-        __syncthreads();
-        if (middle) {
 #pragma unroll
             for (int q = 0; q < SB; q++) buf[(i * SB + q) * G + gi] = v[q];
         }
-        __syncthreads();
+        f2_compute_bar();
         // inverse pass 2 (radix SA, items i < SB), twiddle, store
         if (outer) {
-            float2* row = row_ptr(j);
+            float2 u[SA];
 #pragma unroll
             for (int q = 0; q < SA; q++) {
                 const float2 x = buf[(i + q * SB) * G + gi];
@@ -578,18 +600,21 @@ __global__ void __launch_bounds__(kF2Threads, 1)
                 }
             }
             RegDft<SA, true>::run(u);
+            if (ok) {
+                float2* row = row_ptr(j);
 #pragma unroll
-            for (int q = 0; q < SA; q++) {
-                const int n2 = i + q * SB;
-                float2 w = tw[n2];
-                w.y = -w.y;
-                row[n2 * G + gi] = cmul(u[q], w);
+                for (int q = 0; q < SA; q++) {
+                    const int n2 = i + q * SB;
+                    float2 w = tw[n2];
+                    w.y = -w.y;
+                    row[n2 * G + gi] = cmul(u[q], w);
+                }
             }
         }
         // the slot's generic-proxy accesses are ordered before the next bulk copy into it
         tc::fence_proxy_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0 && j + kF2Ring < mine) issue(j + kF2Ring);
+        __syncwarp();
+        if ((t & 31) == 0) tc::mbar_arrive(&empty[j % kF2Ring]);
     }
 }
 
