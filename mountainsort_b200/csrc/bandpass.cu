@@ -313,27 +313,32 @@ __device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geo
 // Global loads feed pass 1 directly and pass 2 stores directly.
 
 // F1, forward columns of length L1 = RA * RB.
-template <int RA, int RB>
+// LG >= 0 and KL2 > 0 fix log2 G and L2 at compile time (the canonical
+// window with 16 signals per unit), so the index arithmetic folds into
+// constant offsets; LG = -1 reads them from g.
+template <int RA, int RB, int LG, int KL2>
 __global__ void __launch_bounds__(256, 3) bpr_cols_forward(const void* __restrict__ raw, float2* __restrict__ scratch,
                                                         Geom g, const float2* __restrict__ roots, int64_t unit0) {
     constexpr int n = RA * RB;
+    const int lg = LG >= 0 ? LG : g.log2G;
+    const int64_t L2 = KL2 > 0 ? KL2 : g.L2;
     extern __shared__ float4 smem_f4[];
     float2* buf = reinterpret_cast<float2*>(smem_f4);
-    float2* rt = buf + ((size_t)n << g.log2G);
+    float2* rt = buf + ((size_t)n << lg);
     for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
-    const int G = 1 << g.log2G;
+    const int G = 1 << lg;
     const int n2 = blockIdx.x;
     const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
     const int64_t t0 = ui.c * g.chunk - kOverlap + n2;
     const int64_t s0 = (int64_t)ui.grp * G;
     // interior window of whole channel pairs: plain strided loads, no checks
-    const bool interior = g.paired && g.m_even && s0 + G <= g.P && t0 >= 0 && t0 + (int64_t)(n - 1) * g.L2 < g.N;
-    for (int it = threadIdx.x; it < (RB << g.log2G); it += blockDim.x) {
-        const int gi = it & (G - 1), i = it >> g.log2G;
+    const bool interior = g.paired && g.m_even && s0 + G <= g.P && t0 >= 0 && t0 + (int64_t)(n - 1) * L2 < g.N;
+    for (int it = threadIdx.x; it < (RB << lg); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> lg;
         float2 u[RA];
         if (interior) {
-            const int64_t row0 = (t0 + (int64_t)i * g.L2) * g.M;
-            const int64_t step = (int64_t)RB * g.L2 * (g.M / 2);  // pairs per RB window rows
+            const int64_t row0 = (t0 + (int64_t)i * L2) * g.M;
+            const int64_t step = (int64_t)RB * L2 * (g.M / 2);  // pairs per RB window rows
             if (g.in_i16) {
                 const short2* p = reinterpret_cast<const short2*>(static_cast<const int16_t*>(raw) + row0) + (s0 + gi);
 #pragma unroll
@@ -348,25 +353,25 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_forward(const void* __restric
             }
         } else {
 #pragma unroll
-            for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * g.L2, s0 + gi);
+            for (int q = 0; q < RA; q++) u[q] = load_signal(raw, g, t0 + (int64_t)(i + q * RB) * L2, s0 + gi);
         }
         RegDft<RA, false>::run(u);
 #pragma unroll
-        for (int q = 0; q < RA; q++) buf[((i * RA + q) << g.log2G) + gi] = u[q];
+        for (int q = 0; q < RA; q++) buf[((i * RA + q) << lg) + gi] = u[q];
     }
     __syncthreads();
     float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
-    for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
-        const int gi = it & (G - 1), i = it >> g.log2G;
+    for (int it = threadIdx.x; it < (RA << lg); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> lg;
         float2 u[RB];
 #pragma unroll
         for (int q = 0; q < RB; q++) {
-            const float2 v = buf[((i + q * RA) << g.log2G) + gi];
+            const float2 v = buf[((i + q * RA) << lg) + gi];
             u[q] = (q == 0) ? v : cmul(v, rt[q * i]);
         }
         RegDft<RB, false>::run(u);
-        float2* o = slab + (((size_t)i * g.L2 + n2) << g.log2G) + gi;
-        const size_t step = ((size_t)RA * g.L2) << g.log2G;
+        float2* o = slab + (((size_t)i * L2 + n2) << lg) + gi;
+        const size_t step = ((size_t)RA * L2) << lg;
 #pragma unroll
         for (int q = 0; q < RB; q++) o[q * step] = u[q];
     }
@@ -620,21 +625,24 @@ __global__ void __launch_bounds__(kF2Threads, 1)
 
 // F3, inverse columns of length L1 = RA * RB (inverse order: radix RB, then
 // radix RA), trim / subsample / quantize, store.
-template <int RA, int RB>
+// LG, KL2 as for bpr_cols_forward.
+template <int RA, int RB, int LG, int KL2>
 __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restrict__ scratch, void* __restrict__ out,
                                                         Geom g, const float2* __restrict__ roots, int64_t unit0,
                                                         int direct_ok) {
     constexpr int n = RA * RB;
+    const int lg = LG >= 0 ? LG : g.log2G;
+    const int64_t L2v = KL2 > 0 ? KL2 : g.L2;
     extern __shared__ float4 smem_f4[];
     float2* buf = reinterpret_cast<float2*>(smem_f4);
-    float2* rt = buf + ((size_t)n << g.log2G);
+    float2* rt = buf + ((size_t)n << lg);
     for (int i = threadIdx.x; i < n; i += blockDim.x) rt[i] = roots[i];
-    const int G = 1 << g.log2G;
+    const int G = 1 << lg;
     const int n2 = blockIdx.x;
     const UnitIdx ui = unit_index(g, unit0 + blockIdx.y);
     const int64_t s0 = (int64_t)ui.grp * G;
     const int64_t ot_base = (ui.c * g.chunk) / g.sub;
-    const int L2 = (int)g.L2;
+    const int L2 = (int)L2v;
     // float output of whole channel pairs, no subsampling, the whole chunk
     // inside the output: the kept window rows n1 in [60000 / L2, (60000 +
     // chunk) / L2) are exactly q in [kQ0, kQ1) for every item i < RB (checked
@@ -643,24 +651,24 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restr
     const bool direct = direct_ok && g.sub == 1 && !g.out_i16 && g.paired && g.m_even && s0 + G <= g.P &&
                         (ui.c + 1) * g.chunk <= g.N2;
     const float2* slab = scratch + (size_t)blockIdx.y * (size_t)(g.L * G);
-    for (int it = threadIdx.x; it < (RA << g.log2G); it += blockDim.x) {
-        const int gi = it & (G - 1), i = it >> g.log2G;
+    for (int it = threadIdx.x; it < (RA << lg); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> lg;
         float2 u[RB];
-        const float2* p = slab + (((size_t)i * g.L2 + n2) << g.log2G) + gi;
-        const size_t step = ((size_t)RA * g.L2) << g.log2G;
+        const float2* p = slab + (((size_t)i * L2v + n2) << lg) + gi;
+        const size_t step = ((size_t)RA * L2v) << lg;
 #pragma unroll
         for (int q = 0; q < RB; q++) u[q] = p[q * step];
         RegDft<RB, true>::run(u);
 #pragma unroll
-        for (int q = 0; q < RB; q++) buf[((i * RB + q) << g.log2G) + gi] = u[q];
+        for (int q = 0; q < RB; q++) buf[((i * RB + q) << lg) + gi] = u[q];
     }
     __syncthreads();
-    for (int it = threadIdx.x; it < (RB << g.log2G); it += blockDim.x) {
-        const int gi = it & (G - 1), i = it >> g.log2G;
+    for (int it = threadIdx.x; it < (RB << lg); it += blockDim.x) {
+        const int gi = it & (G - 1), i = it >> lg;
         float2 u[RA];
 #pragma unroll
         for (int q = 0; q < RA; q++) {
-            const float2 x = buf[((i + q * RB) << g.log2G) + gi];
+            const float2 x = buf[((i + q * RB) << lg) + gi];
             if (q == 0) {
                 u[q] = x;
             } else {
@@ -694,6 +702,7 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restr
 // (chunk 120000, L = 240000 = 480 x 500, used whenever M * T >= 187).
 constexpr int kFastRA = 16, kFastRB = 30;  // L1 = 480
 constexpr int kFastSA = 20, kFastSB = 25;  // L2 = 500
+constexpr int kFastL2 = kFastSA * kFastSB;
 
 // ---------------------------------------------------------------- plans
 
@@ -1020,11 +1029,15 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
             MS3_CUDA(cudaFuncSetAttribute(bp_cols_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             MS3_CUDA(cudaFuncSetAttribute(bp_rows_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             MS3_CUDA(cudaFuncSetAttribute(bp_cols_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_forward<kFastRA, kFastRB>,
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_forward<kFastRA, kFastRB, -1, 0>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_forward<kFastRA, kFastRB, 4, kFastL2>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             MS3_CUDA(cudaFuncSetAttribute(bpr_rows_filter<kFastSA, kFastSB>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_inverse<kFastRA, kFastRB>,
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_inverse<kFastRA, kFastRB, -1, 0>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            MS3_CUDA(cudaFuncSetAttribute(bpr_cols_inverse<kFastRA, kFastRB, 4, kFastL2>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
             MS3_CUDA(cudaFuncSetAttribute(bpr_rows_filter_pipe<kFastSA, kFastSB>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1076,7 +1089,10 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
         dim3 g2((unsigned)plan->L1, (unsigned)nb);
         float2* sc = scratch.as<float2>();
         if (plan->fast) {
-            bpr_cols_forward<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(raw, sc, g, plan->root1, u0);
+            if (g.log2G == 4)
+                bpr_cols_forward<kFastRA, kFastRB, 4, kFastL2><<<g1, 256, fsm1, stream>>>(raw, sc, g, plan->root1, u0);
+            else
+                bpr_cols_forward<kFastRA, kFastRB, -1, 0><<<g1, 256, fsm1, stream>>>(raw, sc, g, plan->root1, u0);
             MS3_LAUNCH_CHECK();
             if (G == F2Pipe<kFastSA, kFastSB>::G && reinterpret_cast<uintptr_t>(sc) % 16 == 0) {
                 const int64_t nrows = nb * plan->L1;
@@ -1088,7 +1104,12 @@ void bandpass_device(const void* raw, int64_t M, int64_t N, void* out, const Ban
                                                                                      plan->kern);
             }
             MS3_LAUNCH_CHECK();
-            bpr_cols_inverse<kFastRA, kFastRB><<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0, direct_ok);
+            if (g.log2G == 4)
+                bpr_cols_inverse<kFastRA, kFastRB, 4, kFastL2>
+                    <<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0, direct_ok);
+            else
+                bpr_cols_inverse<kFastRA, kFastRB, -1, 0>
+                    <<<g1, 256, fsm1, stream>>>(sc, out, g, plan->root1, u0, direct_ok);
             MS3_LAUNCH_CHECK();
         } else {
             bp_cols_forward<<<g1, kThreads, sm1, stream>>>(raw, sc, g, plan->P1, plan->tw1, u0);
