@@ -459,11 +459,12 @@ __global__ void __launch_bounds__(320) bpr_rows_filter(float2* __restrict__ scra
 }
 
 // F2, pipelined: the same arithmetic as bpr_rows_filter (bit-identical
-// results) in a persistent CTA per SM that walks rows r = blockIdx.x +
-// j * gridDim.x.  A copy warp brings each row (L2 x 16 complex values, 64000
-// bytes), its twiddle row and its kernel row by 1-D bulk copies into a ring
-// of kF2Ring shared-memory slots, one row ahead of the compute warps, and
-// refills a slot as soon as the 13 compute warps have released it.  The three
+// results) in a persistent CTA per SM that walks rows nrows - 1 - r,
+// r = blockIdx.x + j * gridDim.x.  A copy warp brings each row (L2 x 16
+// complex values, 64000 bytes), its twiddle row and its kernel row by 1-D
+// bulk copies into a ring of kF2Ring shared-memory slots, one row ahead of
+// the compute warps, and refills a slot as soon as the 13 compute warps have
+// released it.  The three
 // register passes ping-pong between the slot and one transfer buffer (slot ->
 // transfer -> slot), so a row needs only two barriers of the compute warps
 // (named barrier 1): one after each exchange.  A failed wait sets the error
@@ -508,8 +509,13 @@ __global__ void __launch_bounds__(kF2Threads, 1)
     const int64_t L1 = g.L1;
     const int64_t mine = (blockIdx.x < nrows) ? (nrows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     auto slot_ptr = [&](int64_t j) { return smem + (size_t)(j % kF2Ring) * P::kSlotBytes; };
+    // rows in reverse order of the batch: the forward-column pass wrote the
+    // last units most recently, so the first rows read here are still in L2
+    // (and the inverse-column pass, which walks the units forward, finds the
+    // first units this pass wrote last)
+    auto row_of = [&](int64_t j) { return nrows - 1 - (blockIdx.x + j * gridDim.x); };
     auto row_ptr = [&](int64_t j) {
-        const int64_t r = blockIdx.x + j * gridDim.x;
+        const int64_t r = row_of(j);
         return scratch + (size_t)(r / L1) * (size_t)(g.L * G) + (size_t)(r % L1) * (n * G);
     };
     if (threadIdx.x == 0) {
@@ -530,7 +536,7 @@ __global__ void __launch_bounds__(kF2Threads, 1)
                 if (j >= kF2Ring &&
                     !tc::mbar_wait(&empty[j % kF2Ring], (uint32_t)(((j / kF2Ring) - 1) & 1), err))
                     break;
-                const int64_t k1 = (blockIdx.x + j * gridDim.x) % L1;
+                const int64_t k1 = row_of(j) % L1;
                 uint8_t* slot = slot_ptr(j);
                 uint64_t* bar = &full[j % kF2Ring];
                 tc::mbar_expect_tx(bar, P::kSlotBytes);
