@@ -6,8 +6,9 @@ all-gather).
 
 Gates: every rank's filtered timepoints equal the one-GPU call's bit for
 bit; one rank gives the one-GPU whitened output bit for bit; 2 and 3 ranks
-agree with it to relative L2 <= 1e-6 (the FP64 covariance grouping) and with
-ref32 to <= 1e-5."""
+agree with it to relative L2 <= 1e-6 below 128 channels (the FP64
+covariance grouping) and <= 1e-5 from 128 channels (each rank's tensor-core
+covariance starts its own runs), and with ref32 to <= 1e-5."""
 import os
 import socket
 import sys
