@@ -11,6 +11,9 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libms3gpu.so")
+# the bounds-checked build (python -m mountainsort_b200.build --checked);
+# MS3GPU_LIBRARY=checked makes load() use it
+CHECKED_LIB_PATH = os.path.join(HERE, "libms3gpu_checked.so")
 
 OK = 0
 ERR_INVALID = -1
@@ -127,9 +130,12 @@ SIGNATURES = {
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load the library (once).  Raises OSError if it is missing."""
+def load(path: str = None):
+    """Load the library (once): libms3gpu.so, or libms3gpu_checked.so when
+    MS3GPU_LIBRARY=checked.  Raises OSError if it is missing."""
     global _lib
+    if path is None:
+        path = CHECKED_LIB_PATH if os.environ.get("MS3GPU_LIBRARY") == "checked" else LIB_PATH
     if _lib is None:
         if not os.path.exists(path):
             raise OSError(f"libms3gpu.so not built: {path} (run python -m mountainsort_b200.build)")

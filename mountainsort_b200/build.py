@@ -2,6 +2,7 @@
 in-tree, next to this file.
 
     python -m mountainsort_b200.build        # or build() from Python
+    python -m mountainsort_b200.build --no-checked   # without libms3gpu_checked.so
 """
 from __future__ import annotations
 
@@ -15,6 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libms3gpu.so")
+LIB_CHECKED = os.path.join(HERE, "libms3gpu_checked.so")  # -DMS3GPU_BOUNDS_CHECK
 EXE = os.path.join(HERE, "ms3gpu.mp")
 
 CU_SOURCES = ["capi.cu", "bandpass.cu", "whiten.cu", "apply_tc.cu", "pipeline.cu", "stream.cu", "artifacts.cu", "detect.cu", "cov_i8.cu"]
@@ -48,23 +50,37 @@ def _deps():
     return out
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+def _lib_cmd(out: str, checked: bool, ptxas_info: bool):
+    cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-fvisibility=hidden", "-I", INCLUDE, "-I", CSRC, "-DMS3GPU_BUILDING", "-o", out + ".tmp"]
+    if checked:
+        cmd += ["-DMS3GPU_BOUNDS_CHECK"]
+    if ptxas_info:
+        cmd += ["-Xptxas", "-v"]
+    return cmd + [os.path.join(CSRC, s) for s in CU_SOURCES]
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, checked: bool = True) -> str:
+    """Builds libms3gpu.so and, with `checked`, the bounds-checked
+    libms3gpu_checked.so (the two compile at the same time)."""
     deps = _deps()
+    jobs = []
     if force or not _newer(LIB, deps):
-        cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-               "-Xcompiler", "-fvisibility=hidden", "-I", INCLUDE, "-I", CSRC,
-               "-DMS3GPU_BUILDING", "-o", LIB + ".tmp"]
-        if ptxas_info:
-            cmd += ["-Xptxas", "-v"]
-        cmd += [os.path.join(CSRC, s) for s in CU_SOURCES]
+        jobs.append((LIB, _lib_cmd(LIB, False, ptxas_info)))
+    if checked and (force or not _newer(LIB_CHECKED, deps)):
+        jobs.append((LIB_CHECKED, _lib_cmd(LIB_CHECKED, True, False)))
+    procs = []
+    for out, cmd in jobs:
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        procs.append((out, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for out, pr in procs:
+        text, _ = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError("nvcc failed for " + os.path.basename(out) + ":\n" + text)
         if ptxas_info or verbose:
-            print(r.stdout + r.stderr)
-        os.replace(LIB + ".tmp", LIB)
+            print(text)
+        os.replace(out + ".tmp", out)
     if force or not _newer(EXE, deps + [LIB]):
         cmd = [_cxx(), "-O2", "-std=c++17", "-pthread", "-I", INCLUDE, "-I", CSRC, "-o", EXE + ".tmp",
                *[os.path.join(CSRC, s) for s in EXE_SOURCES], "-L", HERE, "-l:libms3gpu.so",
@@ -79,4 +95,5 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)
+    build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv,
+          checked="--no-checked" not in sys.argv)

@@ -135,6 +135,10 @@ __device__ __forceinline__ void emit_row32(float (&y)[32], int lane, uint8_t* st
                                            const CUtensorMap* tmOut, int out_tma, int64_t t, int64_t trow0, int n,
                                            int64_t M, int64_t N, double qunit, int round_1e4,
                                            void* __restrict__ out) {
+    // a float block that starts beyond the last row or column would be clipped
+    // whole: nothing is staged or stored, and the staging ring does not turn
+    // (its bulk-group accounting counts only issued stores)
+    if (out_tma && (n >= M || trow0 >= N)) return;
     if (round_1e4) quantize_1e4_x32(y);
     if (out_tma) {
         uint8_t* stg = staging_warp + (size_t)sbuf * (32 * 128);
@@ -147,7 +151,7 @@ __device__ __forceinline__ void emit_row32(float (&y)[32], int lane, uint8_t* st
         }
         tc::fence_proxy_async_smem();
         __syncwarp();
-        if (lane == 0) {
+        if (lane == 0 && MS3_IN_BOUNDS(n, M, 301) && MS3_IN_BOUNDS(trow0, N, 302)) {
             tc::tma_store_2d(tmOut, stg, n, (int)trow0);
             tc::bulk_commit_group();
         }
@@ -522,6 +526,15 @@ void apply_whitening_tc(const float* X, int64_t M, int64_t N, const double* W, d
     MS3_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
     MS3_CUDA(cudaStreamSynchronize(stream));
     if (herr) throw Error(MS3GPU_ERR_CUDA, "tensor-core apply: pipeline wait timed out");
+}
+
+int bounds_site_apply(cudaStream_t s) {
+#ifdef MS3GPU_BOUNDS_CHECK
+    return take_bounds_site(s);
+#else
+    (void)s;
+    return 0;
+#endif
 }
 
 }  // namespace ms3gpu

@@ -288,6 +288,7 @@ __device__ __forceinline__ void store_filtered(void* __restrict__ out, const Geo
     const int64_t m0 = g.paired ? 2 * s : s;
     const bool has2 = g.paired && (m0 + 1 < g.M);
     const size_t o = (size_t)(ot * g.M + m0);
+    if (!MS3_IN_BOUNDS((int64_t)o + (has2 ? 1 : 0), g.N2 * g.M, 101)) return;
     if (g.out_i16) {
         int16_t* o16 = static_cast<int16_t*>(out);
         o16[o] = x86_float_to_int16((float)((double)v.x * g.qscale));
@@ -372,8 +373,10 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_forward(const void* __restric
         RegDft<RB, false>::run(u);
         float2* o = slab + (((size_t)i * L2 + n2) << lg) + gi;
         const size_t step = ((size_t)RA * L2) << lg;
+        const int64_t e0 = (int64_t)((((size_t)i * L2 + n2) << lg) + gi);
 #pragma unroll
-        for (int q = 0; q < RB; q++) o[q * step] = u[q];
+        for (int q = 0; q < RB; q++)
+            if (MS3_IN_BOUNDS(e0 + (int64_t)(q * step), g.L << lg, 103)) o[q * step] = u[q];
     }
 }
 
@@ -513,7 +516,10 @@ __global__ void __launch_bounds__(kF2Threads, 1)
     // last units most recently, so the first rows read here are still in L2
     // (and the inverse-column pass, which walks the units forward, finds the
     // first units this pass wrote last)
-    auto row_of = [&](int64_t j) { return nrows - 1 - (blockIdx.x + j * gridDim.x); };
+    auto row_of = [&](int64_t j) {
+        const int64_t r = nrows - 1 - (blockIdx.x + j * gridDim.x);
+        return MS3_IN_BOUNDS(r, nrows, 104) ? r : int64_t(0);
+    };
     auto row_ptr = [&](int64_t j) {
         const int64_t r = row_of(j);
         return scratch + (size_t)(r / L1) * (size_t)(g.L * G) + (size_t)(r % L1) * (n * G);
@@ -662,8 +668,10 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restr
         float2 u[RB];
         const float2* p = slab + (((size_t)i * L2v + n2) << lg) + gi;
         const size_t step = ((size_t)RA * L2v) << lg;
+        const int64_t e0 = (int64_t)((((size_t)i * L2v + n2) << lg) + gi);
 #pragma unroll
-        for (int q = 0; q < RB; q++) u[q] = p[q * step];
+        for (int q = 0; q < RB; q++)
+            u[q] = MS3_IN_BOUNDS(e0 + (int64_t)(q * step), g.L << lg, 105) ? p[q * step] : make_float2(0.f, 0.f);
         RegDft<RB, true>::run(u);
 #pragma unroll
         for (int q = 0; q < RB; q++) buf[((i * RB + q) << lg) + gi] = u[q];
@@ -692,8 +700,10 @@ __global__ void __launch_bounds__(256, 3) bpr_cols_inverse(const float2* __restr
                                                       g.M) +
                         (s0 + gi);
             const int64_t step = (int64_t)RB * L2 * (g.M / 2);
+            const int64_t e0 = (ot_base + (int64_t)i * L2 + n2 - kOverlap + (int64_t)kQ0 * RB * L2) * (g.M / 2) + s0 + gi;
 #pragma unroll
-            for (int q = kQ0; q < kQ1; q++) o[(q - kQ0) * step] = u[q];
+            for (int q = kQ0; q < kQ1; q++)
+                if (MS3_IN_BOUNDS(e0 + (q - kQ0) * step, g.N2 * (g.M / 2), 102)) o[(q - kQ0) * step] = u[q];
         } else {
 #pragma unroll
             for (int q = 0; q < RA; q++) {
@@ -1138,6 +1148,15 @@ void bandpass_check_timeout(cudaStream_t stream) {
         MS3_CUDA(cudaStreamSynchronize(stream));
         throw Error(MS3GPU_ERR_CUDA, "bandpass: pipeline wait timed out");
     }
+}
+
+int bounds_site_bandpass(cudaStream_t s) {
+#ifdef MS3GPU_BOUNDS_CHECK
+    return take_bounds_site(s);
+#else
+    (void)s;
+    return 0;
+#endif
 }
 
 }  // namespace ms3gpu

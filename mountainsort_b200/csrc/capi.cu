@@ -180,10 +180,22 @@ int guarded(const char* name, F&& f) {
     return guarded(std::forward<F>(f));
 }
 
+// Bounds-checked build: a recorded index-check failure of any unit becomes
+// this call's error (after the device has finished the call's work).
+void bounds_check_all() {
+#ifdef MS3GPU_BOUNDS_CHECK
+    MS3_CUDA(cudaDeviceSynchronize());
+    const int sites[4] = {bounds_site_bandpass(0), bounds_site_whiten(0), bounds_site_apply(0), bounds_site_cov(0)};
+    for (int v : sites)
+        if (v) throw Error(MS3GPU_ERR_CUDA, "bounds check failed at site " + std::to_string(v));
+#endif
+}
+
 template <class F>
 int guarded(F&& f) {
     try {
         f();
+        bounds_check_all();
         g_last_error.clear();
         return MS3GPU_OK;
     } catch (const Error& e) {

@@ -38,6 +38,45 @@ void count_launch();
         ::ms3gpu::count_launch();         \
     } while (0)
 
+// Index checks of the bounds-checked build (-DMS3GPU_BOUNDS_CHECK, built as
+// libms3gpu_checked.so beside libms3gpu.so by mountainsort_b200.build and
+// loaded by the Python binding when MS3GPU_LIBRARY=checked):
+// MS3_IN_BOUNDS(i, n, site) is true when 0 <= i < n; otherwise it records
+// the first failing site in its translation unit's bounds word and is false,
+// and the caller skips the access, so a wrong index becomes an error status
+// (MS3GPU_ERR_CUDA, "bounds check failed at site ...") instead of a fault.
+// In the ordinary build it is the constant true and costs nothing.
+#ifdef MS3GPU_BOUNDS_CHECK
+static __device__ int g_bounds_site;  // one per translation unit (no relocatable device code)
+__device__ __forceinline__ bool bounds_ok(int64_t i, int64_t n, int site) {
+    if ((uint64_t)i < (uint64_t)n) return true;
+    atomicCAS(&g_bounds_site, 0, site);
+    return false;
+}
+// The translation unit's recorded site (0: none), cleared; synchronizes `s`.
+static inline int take_bounds_site(cudaStream_t s) {
+    int h = 0;
+    if (cudaMemcpyFromSymbolAsync(&h, g_bounds_site, sizeof(int), 0, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return -1;
+    if (h) {
+        const int zero = 0;
+        cudaMemcpyToSymbolAsync(g_bounds_site, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+        cudaStreamSynchronize(s);
+    }
+    return h;
+}
+#define MS3_IN_BOUNDS(i, n, site) ::ms3gpu::bounds_ok((int64_t)(i), (int64_t)(n), (site))
+#else
+#define MS3_IN_BOUNDS(i, n, site) true
+#endif
+// Per translation unit of the library: its recorded bounds-check site, cleared
+// (0 in the ordinary build).
+int bounds_site_bandpass(cudaStream_t s);
+int bounds_site_whiten(cudaStream_t s);
+int bounds_site_apply(cudaStream_t s);
+int bounds_site_cov(cudaStream_t s);
+
 // Stream-ordered device allocation owned by one call.  Freed on the same
 // stream when it goes out of scope, so later work on the stream may not use it.
 class DevBuf {

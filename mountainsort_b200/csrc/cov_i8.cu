@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(256) cov_run_maxbits(const float* __restrict__
         unsigned int m = red[0][threadIdx.x];
         for (int k = 1; k < 8; k++) m = max(m, red[k][threadIdx.x]);
         const int64_t c = (int64_t)blockIdx.y * kB + threadIdx.x;
-        if (m != 0u && c < Mp) atomicMax(maxbits + (t0 / R) * Mp + c, m);
+        if (m != 0u && c < Mp && MS3_IN_BOUNDS((t0 / R) * Mp + c, ((rows + R - 1) / R) * Mp, 402))
+            atomicMax(maxbits + (t0 / R) * Mp + c, m);
     }
 }
 
@@ -402,7 +403,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int64_t c0 = (int64_t)(b ? it.bj : it.bi) * kB + 4 * q;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    int e = run_exponent(__ldg(mb + it.r * Mp + c0 + k));
+                    const int64_t mi = it.r * Mp + c0 + k;
+                    int e = MS3_IN_BOUNDS(mi, nruns * Mp, 403) ? run_exponent(__ldg(mb + mi)) : kSentinel;
                     if (e == kSentinel) e = 0;  // digits are garbage; the drain writes NaN for the channel
                     mult[b][k] = __uint_as_float((uint32_t)(157 - e) << 23);  // 2^(30 - e)
                     m8[b][k] = __uint_as_float((uint32_t)(149 - e) << 23);    // 2^(22 - e)
@@ -484,7 +486,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         v[h] = (ei == kSentinel || ej == kSentinel) ? __longlong_as_double(0x7FF8000000000000LL)
                                                                   : acc * pow2d(ei + ej - 36);
                     }
-                    *reinterpret_cast<double2*>(dst + j0 + jj) = make_double2(v[0], v[1]);
+                    if (MS3_IN_BOUNDS((((int64_t)it.r * P + it.p) * (kB * kB) + (int64_t)row * kB + j0 + jj + 1),
+                                      nruns * P * (kB * kB), 401))
+                        *reinterpret_cast<double2*>(dst + j0 + jj) = make_double2(v[0], v[1]);
                 }
             }
             tc::tc_fence_before();
@@ -630,6 +634,15 @@ void covariance_check_timeout(cudaStream_t stream) {
         throw Error(MS3GPU_ERR_CUDA, "tensor-core covariance: pipeline wait timed out");
     }
     whitening_check_timeout(stream);
+}
+
+int bounds_site_cov(cudaStream_t s) {
+#ifdef MS3GPU_BOUNDS_CHECK
+    return take_bounds_site(s);
+#else
+    (void)s;
+    return 0;
+#endif
 }
 
 }  // namespace ms3gpu

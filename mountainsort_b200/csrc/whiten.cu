@@ -658,7 +658,7 @@ __global__ void gather_channels(const float* __restrict__ X, int64_t M, int64_t 
     const int64_t total = N * M2;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = i / M2, j = i - t * M2;
-        out[i] = X[t * M + ch[j]];
+        if (MS3_IN_BOUNDS(ch[j], M, 201)) out[i] = X[t * M + ch[j]];
     }
 }
 
@@ -670,7 +670,7 @@ __global__ void scatter_channels(const T* __restrict__ Y, int64_t M2, int64_t N,
     const int64_t total = N * M2;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = i / M2, j = i - t * M2;
-        out[t * M + ch[j]] = Y[i];
+        if (MS3_IN_BOUNDS(ch[j], M, 202)) out[t * M + ch[j]] = Y[i];
     }
 }
 
@@ -995,6 +995,15 @@ void apply_whitening_device(const float* X, int64_t M, int64_t N, const double* 
     apply_gemm<<<(unsigned)blocks, 256, 0, stream>>>(X, wt.as<float>(), M, N, quantization_unit, round_1e4 ? 1 : 0,
                                                      out);
     MS3_LAUNCH_CHECK();
+}
+
+int bounds_site_whiten(cudaStream_t s) {
+#ifdef MS3GPU_BOUNDS_CHECK
+    return take_bounds_site(s);
+#else
+    (void)s;
+    return 0;
+#endif
 }
 
 }  // namespace ms3gpu

@@ -32,6 +32,17 @@ def test_library_exports_every_declared_symbol():
     assert set(header_symbols()) == set(_lib.SIGNATURES)
 
 
+def test_bounds_checked_library_exports_the_same_symbols():
+    # the -DMS3GPU_BOUNDS_CHECK twin is built beside the library and loaded
+    # with MS3GPU_LIBRARY=checked; it must offer the same C ABI
+    if not os.path.exists(_lib.CHECKED_LIB_PATH):
+        pytest.skip("libms3gpu_checked.so not built")
+    L = ctypes.CDLL(_lib.CHECKED_LIB_PATH)
+    for s in header_symbols():
+        assert hasattr(L, s), s
+    assert L.ms3gpu_bandpass_chunk_size.restype is not None
+
+
 def test_version_and_geometry():
     L = _lib.load()
     assert b"sm_100a" in L.ms3gpu_version()

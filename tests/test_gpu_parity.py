@@ -83,6 +83,19 @@ def test_bandpass_device_pointers_and_determinism(gpu_lib, rec32):
     np.testing.assert_array_equal(a.cpu().numpy(), h)
 
 
+def test_fused_call_repeats_bit_for_bit_at_16_channels(gpu_lib):
+    """16 channels: the apply's 128-channel tiles have three wholly clipped
+    32-column blocks per row, which are neither staged nor stored; repeated
+    calls must give the same bits (a staging buffer reused while its store
+    still reads it would not)."""
+    import torch
+
+    X = torch.from_numpy(synth.generate_numpy(16, 200_000, K=4, seed=16)).cuda()
+    ref = api.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=16)
+    for _ in range(6):
+        assert torch.equal(api.bandpass_whiten(X, FS, FMIN, FMAX, FWID, num_threads=16), ref)
+
+
 def test_bandpass_no_lowcut(gpu_lib, ref32):
     X = synth.generate_numpy(16, 200000, K=3, seed=11)
     ref = ref32.bandpass_filter(X, FS, 0.0, FMAX, FWID, num_threads=16)
