@@ -14,7 +14,10 @@
 //     A1 = sum d0 d1' + d1 d0'                    (2^40)
 //     A2 = sum d0 d2' + d2 d0' + d1 d1'           (2^32)
 //     A3 = sum d0 d3' + d3 d0' + d1 d2' + d2 d1'  (2^24)
-// (ten MMAs per 32 timepoints; int32 cannot overflow for R <= 32768).  The
+// (ten MMAs per 32 timepoints, seven for a diagonal block pair, whose
+// classes 1 and 3 are computed one half at a time, d0 d1' instead of d0 d1' +
+// d1 d0' = d0 d1' + (d0 d1')^T, the transpose added when the tile is reduced;
+// int32 cannot overflow for R <= 32768).  The
 // classes below 2^24 are dropped; their only non-zero-mean part, the d2 d2
 // term on the diagonal, is added back from per-channel sums of d2^2 kept by
 // the converter threads.  At the end of a run the classes are combined in
@@ -368,16 +371,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                         b[k] = plane_desc(pb + k * kPlaneBytes);
                     }
                     const uint32_t acc0 = (kb != 0);
+                    // a diagonal pair (b = a) skips the transposed halves of
+                    // classes 1 and 3 (d1 d0' = (d0 d1')^T, ...): seven MMAs; the
+                    // drain and the reduction add the transposes back
                     mma_i8(taddr + 0 * kB, a[0], b[0], acc0);
                     mma_i8(taddr + 1 * kB, a[0], b[1], acc0);
-                    mma_i8(taddr + 1 * kB, a[1], b[0], 1);
+                    if (!diag) mma_i8(taddr + 1 * kB, a[1], b[0], 1);
                     mma_i8(taddr + 2 * kB, a[0], b[2], acc0);
                     mma_i8(taddr + 2 * kB, a[2], b[0], 1);
                     mma_i8(taddr + 2 * kB, a[1], b[1], 1);
                     mma_i8(taddr + 3 * kB, a[0], b[3], acc0);
-                    mma_i8(taddr + 3 * kB, a[3], b[0], 1);
+                    if (!diag) mma_i8(taddr + 3 * kB, a[3], b[0], 1);
                     mma_i8(taddr + 3 * kB, a[1], b[2], 1);
-                    mma_i8(taddr + 3 * kB, a[2], b[1], 1);
+                    if (!diag) mma_i8(taddr + 3 * kB, a[2], b[1], 1);
                     tc::mma_commit(&p_empty[s]);
                 }
                 if (ok) tc::mma_commit(acc_full);
@@ -480,9 +486,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int h = 0; h < 2; h++) {
                         const int j = j0 + jj + h;
                         const int ej = run_exponent(__ldg(mbj + j));
-                        double acc = (double)(int)a0[jj + h] * 16777216.0 + (double)(int)a1[jj + h] * 65536.0;
-                        acc += (double)(int)a2[jj + h] * 256.0 + (double)(int)a3[jj + h];
-                        if (diag && j == row) acc += (double)dcorr * 0.00390625;
+                        double acc;
+                        if (!diag) {
+                            acc = (double)(int)a0[jj + h] * 16777216.0 + (double)(int)a1[jj + h] * 65536.0;
+                            acc += (double)(int)a2[jj + h] * 256.0 + (double)(int)a3[jj + h];
+                        } else {
+                            // symmetric classes 0 and 2 (and the d2^2 correction) on and
+                            // above the diagonal; the half classes 1 and 3 everywhere, the
+                            // diagonal's twice: the reduction adds tile(c, r) to tile(r, c)
+                            const double half = (double)(int)a1[jj + h] * 65536.0 + (double)(int)a3[jj + h];
+                            double sym = (double)(int)a0[jj + h] * 16777216.0 + (double)(int)a2[jj + h] * 256.0;
+                            if (j == row) sym += (double)dcorr * 0.00390625;
+                            acc = j > row ? sym + half : (j == row ? sym + 2.0 * half : half);
+                        }
                         v[h] = (ei == kSentinel || ej == kSentinel) ? __longlong_as_double(0x7FF8000000000000LL)
                                                                   : acc * pow2d(ei + ej - 36);
                     }
@@ -522,7 +538,15 @@ __global__ void cov_i8_reduce(const double* __restrict__ partials, int64_t S, in
     if (i >= M || j >= M) return;
     if (bi == bj && c < r) return;  // the diagonal tile's lower half mirrors its upper half
     double s = 0.0;
-    for (int64_t k = 0; k < S; k++) s += partials[((size_t)k * P + p) * (kB * kB) + e];
+    if (bi == bj && c > r) {  // the half classes of the diagonal pair: tile(r, c) + tile(c, r)
+        const int et = c * kB + r;
+        for (int64_t k = 0; k < S; k++) {
+            const double* t = partials + ((size_t)k * P + p) * (kB * kB);
+            s += t[e] + t[et];
+        }
+    } else {
+        for (int64_t k = 0; k < S; k++) s += partials[((size_t)k * P + p) * (kB * kB) + e];
+    }
     if (N > 1) s /= (double)(N - 1);
     XXt[i + M * j] = s;
     XXt[j + M * i] = s;
