@@ -139,15 +139,22 @@ def _signals(M, N, seed):
 def test_digits_reconstruct_the_fixed_point_value():
     rng = np.random.default_rng(1)
     x = (rng.standard_normal(20000) * 3.0).astype(np.float32)
-    # values whose x 2^(22-e) falls on a half: rounding to even leaves a remainder of +128
-    x[:8] = np.float32(2.0) ** -5 * np.array([129, 131, 133, 135, 137, 139, 141, 143], np.float32) / np.float32(128)
-    for e in (run_exponent(x), 4, 7):
+    e0 = run_exponent(x)
+    # values whose x 2^(22-e) falls on a half: where rounding to even goes down
+    # the remainder is +128, which a byte cannot hold, and is held at 127
+    n = np.arange(8)
+    x[:8] = ((2 * n + 1) * 2.0 ** (e0 - 23)).astype(np.float32)
+    assert run_exponent(x) == e0
+    for e in (e0, e0 + 3, 40):
         d, v = digits(x, e)
         assert np.abs(d[0]).max() <= 64
         for k in (1, 2, 3):
             assert d[k].min() >= -128 and d[k].max() <= 127
         assert np.array_equal(v, d[0] * 2**24 + d[1] * 2**16 + d[2] * 2**8 + d[3])
-        assert np.abs(v - x.astype(np.float64) * 2.0 ** (30 - e)).max() <= 1.0
+        xs = x.astype(np.float64) * 2.0 ** (30 - e)
+        assert np.abs(v - xs).max() <= 1.0
+        if e == e0:
+            assert np.array_equal(xs[:8] - v[:8], np.where(n % 2 == 0, 1.0, 0.0))
 
 
 @pytest.mark.parametrize("M,N,R", [(130, 40000, 8192), (128, 20001, 8192), (8, 5000, 1024)])
