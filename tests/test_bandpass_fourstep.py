@@ -13,7 +13,10 @@ frequency k = k1 + L1 k2:
 and carries two real channels as one complex signal x_a + i x_b, which is
 exact because the band kernel is real and even (kernel[k] = kernel[L - k]):
 the real and imaginary parts of the filtered signal are the two filtered
-channels.  These tests check the index algebra and the pairing, not the GPU:
+channels.  A window length with a prime factor above 64 is filtered as a
+zero-padded circular convolution of a 5-smooth length P >= 2L - 1, which
+equals the length-L circular filter because the taps are even.  These tests
+check the index algebra, the pairing and the padding, not the GPU:
 the GPU passes are checked against the oracle in tests/test_gpu_parity.py."""
 import numpy as np
 import pytest
@@ -93,3 +96,56 @@ def test_pairing_needs_an_even_kernel():
     y = four_step_filter((x[:, 0] + 1j * x[:, 1])[:, None], kern, L1, L2)[:, 0]
     ref = direct_filter(x, kern)
     assert o64.rel_l2(y.real, ref[:, 0].real) > 1e-3
+
+
+def _smooth5_at_least(n):
+    """The smallest 2^a 3^b 5^c >= n."""
+    best = None
+    p5 = 1
+    while p5 < 2 * n:
+        p35 = p5
+        while p35 < 2 * n:
+            p = p35
+            while p < n:
+                p *= 2
+            best = p if best is None else min(best, p)
+            p35 *= 3
+        p5 *= 5
+    return best
+
+
+def padded_filter(x, kern):
+    """A window whose length L has a large prime factor: the length-L
+    circular filter as a length-P circular convolution, P >= 2L - 1 and
+    5-smooth, with the taps h = IDFT(kernel) / L laid out as g[j] = g[P - j]
+    = h[j] (the layout of bandpass.cu's padded plans).  g is real and even,
+    so its P-point spectrum is real and even and pairs of channels still
+    travel as one complex signal."""
+    L = x.shape[0]
+    P = _smooth5_at_least(2 * L - 1)
+    h = np.fft.ifft(kern).real
+    g = np.zeros(P)
+    g[:L] = h
+    g[P - L + 1:] = h[1:][::-1]
+    G = np.fft.fft(g)
+    assert np.abs(G.imag).max() <= 1e-12 * np.abs(G.real).max()
+    xp = np.zeros((P,) + x.shape[1:], dtype=np.result_type(x, np.complex128))
+    xp[:L] = x
+    return np.fft.ifft(np.fft.fft(xp, axis=0) * G.real[:, None], axis=0)[:L]
+
+
+def test_smooth5_lengths():
+    assert [_smooth5_at_least(n) for n in (1, 7, 11, 97, 932065)] == [1, 8, 12, 100, 933120]
+
+
+@pytest.mark.parametrize("L", [1009, 466033])
+def test_padded_window_equals_the_circular_filter(ref32, L):
+    # 466033 (prime) is the window of 6 channels at 16 threads
+    kern = ref32.define_kernel(L, 30000.0, 300.0, 6000.0, 1000.0)
+    rng = np.random.default_rng(L)
+    x = rng.standard_normal((L, 2)) * 50.0
+    z = x[:, 0] + 1j * x[:, 1]
+    y = padded_filter(z[:, None], kern)[:, 0]
+    ref = direct_filter(x, kern).real
+    assert o64.rel_l2(y.real, ref[:, 0]) < 1e-12
+    assert o64.rel_l2(y.imag, ref[:, 1]) < 1e-12
