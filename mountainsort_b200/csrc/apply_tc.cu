@@ -64,9 +64,10 @@ struct TcCfg {
 
 // The reference's 1e-4 rounding, floor(x / 1e-4 + 0.5) * 1e-4 in double
 // (p_whiten.cpp:185-189), for 32 values in place.  x * 10000 stands in for
-// the division except within 1e-6 of a rounding boundary, where the two can
-// differ; those (rare) values are redone with the division in a second loop,
-// so the main loop has no branch and its 32 chains interleave.
+// the division: for a float x it is exact in double and the quotient rounds
+// to the same double (it lies within 0.43 ulp of it).  As a guard, values
+// within 1e-6 of a rounding boundary are redone with the division in a
+// second loop, so the main loop has no branch and its 32 chains interleave.
 __device__ __forceinline__ void quantize_1e4_x32(float (&y)[32]) {
 #pragma unroll
     for (int h = 0; h < 32; h += 16) {  // two halves keep the live registers down

@@ -575,9 +575,10 @@ __global__ void w_to_float(const double* __restrict__ W, int64_t MM, float* __re
 }
 
 // quantize(x, 1e-4) = floor(x/1e-4 + 0.5) * 1e-4 in double (p_whiten.cpp:31-41).
-// x * 1e4 differs from x / 1e-4 by at most a few ulps, so its floor is used
-// unless the value sits within 1e-6 of a rounding boundary, where the exact
-// IEEE division decides.
+// For a float x, x * 1e4 is exact in double (at most 34 significant bits)
+// and the quotient x / 0.0001 lies within 0.43 ulp of it (the double 0.0001
+// is 1e-4 (1 + 4.8e-17)), so the two are the same double; the division is
+// kept as a guard for values within 1e-6 of a rounding boundary.
 __device__ __forceinline__ float quantize_1e4(float x) {
     const double xd = (double)x;
     double t = __dadd_rn(__dmul_rn(xd, 10000.0), 0.5);
