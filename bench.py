@@ -38,8 +38,8 @@ UNIT = "Gch-samples/s"
 
 SIZES = {
     # name: (M, N, units, description)
-    "c2": (384, 18_000_000, 300, "384ch x 18M timepoints (10 min @ 30 kHz), config 2"),
-    "c1": (32, 1_800_000, 20, "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1"),
+    "c2": (384, 18_000_000, 300, "384ch x 18M timepoints (10 min @ 30 kHz), plain FP32 form"),
+    "c1": (32, 1_800_000, 20, "32ch x 1.8M timepoints (60 s @ 30 kHz), CPU-runnable size"),
     "small": (384, 600_000, 20, "384ch x 600k timepoints (20 s @ 30 kHz), profiling case"),
 }
 
@@ -253,7 +253,7 @@ def reference_c1_full(threads):
         if L.msref_whiten(pf.encode(), pp.encode(), 0.0, threads) != 0:
             return None
         t2 = time.perf_counter()
-        return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1, timed in full",
+        return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz), timed in full",
                 "value": M * N / (t2 - t0) / 1e9, "unit": UNIT, "seconds": t2 - t0,
                 "bandpass_s": t1 - t0, "whiten_s": t2 - t1, "kind": "reference", "cores": threads,
                 "geometry_threads": GEOM_T}
@@ -292,7 +292,7 @@ def run_reference_arm(args, size):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "timing": ("ms_per_step is the wall time of one measured sample (see cpu_baseline.sample); value is "
                    "the recording's throughput from those measurements"),
-        "config1_full": c1,
+        "cpu_size_full": c1,
         "wall_s": time.perf_counter() - t_start,
     }
     print(json.dumps(line), flush=True)
@@ -354,7 +354,7 @@ def mixed_record(ms, synth, dev, stream):
                                                    precision="mixed"), stream, 5)
     pre_mixed = out.cpu().numpy()
     _, q64, _, _ = oracle64.whiten(oracle64.bandpass_filter(Xh, FS, FMIN, FMAX, FWID, num_threads=GEOM_T))
-    return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz), config 1 data",
+    return {"workload": "32ch x 1.8M timepoints (60 s @ 30 kHz) data",
             "plain_ms": t_plain, "mixed_ms": t_mixed, "plain_gchs": M * N / t_plain / 1e6,
             "mixed_gchs": M * N / t_mixed / 1e6, "mixed_over_plain": t_plain / t_mixed,
             "mixed_rel_l2_vs_fp64": oracle64.rel_l2(pre_mixed, q64),
@@ -640,7 +640,7 @@ def main():
                      "unit": "GB/s", "peak_source": peak_src}
     step_roofline["frac"] = step_roofline["achieved"] / hbm_peak
 
-    # ---- mixed-precision form on the config-1 data, next to the plain form (FP64 oracle for its error)
+    # ---- mixed-precision form on the 32ch x 1.8M data, next to the plain form (FP64 oracle for its error)
     mixed = None
     if rank == 0 and not args.no_mixed:
         mixed = mixed_record(ms, synth, dev, stream)

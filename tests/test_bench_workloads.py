@@ -9,7 +9,7 @@ sys.path.insert(0, ROOT)
 import bench  # noqa: E402
 
 
-def test_headline_and_config1_sizes():
+def test_headline_and_cpu_size_workloads():
     assert bench.SIZES["c2"][:2] == (384, 18_000_000)  # 10 min at 30 kHz
     assert bench.SIZES["c1"][:2] == (32, 1_800_000)    # 60 s at 30 kHz
     assert (bench.FS, bench.FMIN, bench.FMAX, bench.FWID) == (30000.0, 300.0, 6000.0, 1000.0)

@@ -234,7 +234,7 @@ def test_apply_plain_and_mixed_at_384(gpu_lib, ref32):
 
 
 def test_mixed_pipeline_vs_fp64_oracle(gpu_lib, rec32):
-    # the mixed-precision form on config-1 geometry, gated against the FP64 oracle
+    # the mixed-precision form on the 32ch x 1.8M geometry, gated against the FP64 oracle
     pre = api.bandpass_whiten(rec32, FS, FMIN, FMAX, FWID, num_threads=16, precision="mixed")
     y, q64, _, _ = o64.whiten(o64.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16))
     err = rel(pre, q64)
@@ -251,7 +251,7 @@ def test_whiten_int16(gpu_lib, ref32, rec32):
     assert d.max() <= 1 and np.mean(d) < 1e-3
 
 
-def test_fused_pipeline_config1_geometry(gpu_lib, ref32, rec32):
+def test_fused_pipeline_32ch_geometry(gpu_lib, ref32, rec32):
     """ms3.bandpass_filter then ms3.whiten, as mountainsort3.mlp runs them."""
     filt_ref = ref32.bandpass_filter(rec32, FS, FMIN, FMAX, FWID, num_threads=16)
     pre_ref, _, _ = ref32.whiten(filt_ref)
