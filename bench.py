@@ -230,8 +230,8 @@ def cpu_baseline(M: int, N: int, threads: int):
 
 
 def reference_c1_full(threads):
-    """Configuration 1 (32 x 1.8M, 60 s at 30 kHz) run in full through the
-    reference's own processors, file to file: bandpass then whiten."""
+    """The CPU-runnable size (32 x 1.8M, 60 s at 30 kHz) run in full through
+    the reference's own processors, file to file: bandpass then whiten."""
     import numpy as np
 
     from mountainsort_b200 import mdaio, synth
