@@ -192,3 +192,43 @@ def test_digit_covariance_edge_channels():
     assert np.all(np.isnan(C[40])) and np.all(np.isnan(C[:, 40]))
     keep = np.setdiff1d(np.arange(M), [40])
     assert o64.rel_l2(C[np.ix_(keep, keep)], o64.xxt(X[:, keep])) <= 1e-8
+
+
+def digits_from_bit_patterns(x, e):
+    """digits4 and convert_stage as the converter warps compute them, in
+    float32 and uint32: y1 = x 2^(22-e) + 1.5 2^23 (one rounding: the product
+    is exact, and the FP64 sum is exact for every input, so its cast is the
+    fma's rounding), vh = y1 - 1.5 2^23, rem = min(vh (-256) + x 2^(30-e),
+    127) (exact), y2 = rem + 1.5 2^23; w = bits(y1) - 0x3F7F80, lo = bits(y2);
+    d0 = byte 2 of w, d1 = byte 1 ^ 0x80, d2 = byte 0 ^ 0x80, d3 = byte 0 of
+    lo, each read as a signed byte."""
+    x = np.asarray(x, np.float32)
+    m8 = np.float32(2.0 ** (22 - e))
+    m = np.float32(2.0 ** (30 - e))
+    c = np.float32(12582912.0)
+    y1 = (x.astype(np.float64) * np.float64(m8) + 12582912.0).astype(np.float32)
+    vh = y1 - c
+    xm = x * m
+    rem = np.minimum((vh.astype(np.float64) * -256.0 + xm.astype(np.float64)).astype(np.float32), np.float32(127.0))
+    y2 = rem + c
+    w = (y1.view(np.uint32).astype(np.int64) - 0x3F7F80) & 0xFFFFFFFF
+    lo = y2.view(np.uint32).astype(np.int64)
+
+    def sbyte(b):
+        return ((b & 0xFF) ^ 0x80) - 0x80
+
+    return [sbyte(w >> 16), sbyte(((w >> 8) & 0xFF) ^ 0x80), sbyte((w & 0xFF) ^ 0x80), sbyte(lo)]
+
+
+def test_kernel_bit_patterns_give_the_digits():
+    rng = np.random.default_rng(7)
+    x = (rng.standard_normal(400000) * np.exp(rng.uniform(-12, 12, 400000))).astype(np.float32)
+    x[:4] = [0.0, -0.0, np.float32(1e-40), np.float32(-3e-39)]
+    for e in sorted({run_exponent(x), run_exponent(x[: 1000]), -20, 0, 9}):
+        xx = x[np.abs(x.astype(np.float64)) < 2.0 ** e]  # the run's values lie below 2^e
+        n = np.arange(min(16, xx.size))
+        xx[: n.size] = ((2 * n + 1) * 2.0 ** (e - 23) * np.where(n % 2, -1, 1)).astype(np.float32)  # ties
+        got = digits_from_bit_patterns(xx, e)
+        want, _ = digits(xx, e)
+        for k in range(4):
+            assert np.array_equal(got[k], want[k]), (e, k)
