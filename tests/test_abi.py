@@ -52,6 +52,14 @@ def test_version_and_geometry():
     assert L.ms3gpu_bandpass_chunk_size(0, 16) == -1
 
 
+def test_chunk_size_matches_the_oracle_on_a_grid(ref32):
+    # the window geometry of every (channels, threads) the reference can be run with
+    # (p_bandpass_filter.cpp:147-155): the output depends on it beyond any tolerance
+    for M in list(range(1, 70)) + [96, 127, 128, 129, 192, 255, 256, 383, 384, 385, 512, 1024, 1536, 4096]:
+        for T in (1, 2, 3, 7, 8, 15, 16, 27, 32, 63, 64, 128):
+            assert api.chunk_size(M, T) == ref32.chunk_size(M, T), (M, T)
+
+
 def test_output_dims():
     L = _lib.load()
     M, N, dt = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
